@@ -1,0 +1,144 @@
+/*
+ * tilestream_c.h - the C entry points of libtilestream_b200.so.
+ *
+ * A flat C ABI over the drop-in C++ API of include/tilestream/ (plain pointers, sizes and POD
+ * records; no C++ or torch types). Every record below has exactly the layout of the C++ record
+ * it mirrors (checked with static_asserts in the library), and every function returns the
+ * reference's Status value (include/tilestream/types.h: 0 = success ... 10 = io_error).
+ * Streams are CUDA stream handles (cudaStream_t) passed as void*.
+ *
+ * Each declaration names the reference interface it replaces (path:line in the reference).
+ */
+#ifndef TILESTREAM_C_H
+#define TILESTREAM_C_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- records (include/tilestream/types.h:21-71, cuda.h:16-109) ------------------------- */
+typedef struct { uint32_t type, width, height; } ts_image_spec;    /* ImageSpec */
+typedef struct { uint16_t width, height; } ts_tile_shape;         /* TileShape */
+typedef struct { uint32_t x, y, width, height; } ts_roi;          /* Roi */
+typedef struct { const void *data; uint64_t size; } ts_const_bytes;
+typedef struct { void *data; uint64_t size; } ts_mutable_bytes;
+typedef struct {
+    const void *data;
+    ts_image_spec image;
+    uint64_t pitch_bytes, capacity_bytes;
+} ts_const_image_view;
+typedef struct {
+    void *data;
+    ts_image_spec image;
+    uint64_t pitch_bytes, capacity_bytes;
+} ts_image_view;
+typedef struct { uint32_t status, reserved; uint64_t bytes_written; } ts_device_result;
+typedef struct { uint32_t kind; float scalar; ts_const_image_view map; } ts_parameter;
+typedef struct { ts_parameter offset, gain; } ts_calibration;
+typedef struct { uint64_t tile_index, input_offset; } ts_tile_mapping;
+typedef struct { uint64_t file_bytes, tile_count, metadata_bytes; } ts_parse_limits;
+typedef struct {
+    uint64_t image_count, tile_count;
+    ts_tile_shape tile;
+    uint64_t scan_temp_bytes;
+} ts_workspace_spec;
+/* Host metadata tables (api.h:11-35): TileMetadata is 32 bytes, SegmentMetadata 24 bytes. */
+typedef struct {
+    uint32_t mode;
+    uint16_t width, height;
+    uint64_t offset, length, first_segment;
+} ts_tile_metadata;
+typedef struct {
+    uint32_t seed, bit_width;
+    uint64_t payload_offset, payload_bytes;
+} ts_segment_metadata;
+
+/* An owned tilestream::ImageMetadata (api.h:29-35). */
+typedef struct ts_metadata ts_metadata;
+/* An owned tilestream::cuda::BatchPlan (cuda.h:148-174). */
+typedef struct ts_plan ts_plan;
+
+typedef struct {
+    ts_const_bytes bytes;
+    const ts_metadata *metadata;
+    const ts_tile_mapping *mappings;
+    uint64_t mapping_count;
+    const ts_device_result *encoder_result;
+    ts_image_spec trusted_image;
+    ts_tile_shape trusted_tile;
+} ts_compressed_input; /* CompressedInput, cuda.h:42-51 */
+typedef struct {
+    ts_const_image_view input;
+    ts_image_view output;
+    ts_mutable_bytes compressed_output;
+    ts_compressed_input compressed_input;
+    ts_roi roi;
+    ts_calibration calibration;
+} ts_batch_item; /* BatchItem, cuda.h:53-60 */
+typedef struct {
+    uint32_t operation; /* 0 compress, 1 decompress, 2 decode_roi, 3 calibrate, 4 decode_calibrate */
+    const ts_batch_item *items;
+    uint64_t count;
+    ts_tile_shape tile;
+} ts_batch_request; /* BatchRequest, cuda.h:62-67 */
+typedef struct { ts_device_result *data; uint64_t count; } ts_result_buffer; /* cuda.h:106-109 */
+
+/* ---- size queries (sizing.h:26-30) ------------------------------------------------------ */
+int ts_image_span(ts_image_spec image, uint64_t pitch_bytes, uint64_t *bytes);
+int ts_compress_bound(ts_image_spec image, ts_tile_shape tile, uint64_t *bytes);
+int ts_workspace_size(const ts_workspace_spec *spec, uint64_t *bytes);
+
+/* ---- host parser (api.h:42-43) ------------------------------------------------------------
+ * On success *out receives a new handle (free with ts_metadata_destroy); on failure *out is
+ * left unchanged. limits may be NULL for no budget. */
+int ts_parse_metadata(ts_const_bytes source, const ts_parse_limits *limits, ts_metadata **out);
+/* Wraps caller-built tables (copied) as metadata for a GPU plan. */
+int ts_metadata_create(ts_image_spec image, ts_tile_shape tile, uint64_t file_bytes,
+                       const ts_tile_metadata *tiles, uint64_t tile_count,
+                       const ts_segment_metadata *segments, uint64_t segment_count,
+                       ts_metadata **out);
+void ts_metadata_destroy(ts_metadata *metadata);
+void ts_metadata_info(const ts_metadata *metadata, ts_image_spec *image, ts_tile_shape *tile,
+                      uint64_t *file_bytes, uint64_t *tile_count, uint64_t *segment_count);
+const ts_tile_metadata *ts_metadata_tiles(const ts_metadata *metadata);
+const ts_segment_metadata *ts_metadata_segments(const ts_metadata *metadata);
+
+/* ---- CPU codec (cpu.h:9-12) ---------------------------------------------------------------- */
+int ts_cpu_compress(ts_const_image_view input, ts_tile_shape tile, ts_mutable_bytes output,
+                    uint64_t *bytes_written);
+int ts_cpu_decompress(ts_const_bytes input, ts_image_view output, const ts_parse_limits *limits);
+
+/* ---- CUDA plans and executors (cuda.h:176-187) ---------------------------------------------
+ * ts_prepare_batch replaces *plan (destroying the previous plan) only on success. */
+int ts_prepare_batch(const ts_batch_request *request, ts_plan **plan, void *stream);
+void ts_plan_destroy(ts_plan *plan);
+int ts_plan_workspace_spec(const ts_plan *plan, ts_workspace_spec *spec); /* cuda.h:156 */
+int ts_compress_async(const ts_plan *plan, ts_mutable_bytes workspace, ts_result_buffer results,
+                      void *stream);
+int ts_decompress_async(const ts_plan *plan, ts_mutable_bytes workspace, ts_result_buffer results,
+                        void *stream);
+int ts_decode_roi_async(const ts_plan *plan, ts_mutable_bytes workspace, ts_result_buffer results,
+                        void *stream);
+int ts_calibrate_async(const ts_plan *plan, ts_mutable_bytes workspace, ts_result_buffer results,
+                       void *stream);
+int ts_decode_calibrate_async(const ts_plan *plan, ts_mutable_bytes workspace,
+                              ts_result_buffer results, void *stream);
+
+/* ---- device buffers and completion (cuda.h:113-145) ----------------------------------------
+ * Stream-ordered allocation aligned to 256 bytes; *data is replaced only on success. */
+int ts_device_allocate(uint64_t bytes, void *stream, void **data);
+int ts_device_release(void *data, void *stream);
+int ts_synchronize(void *stream);
+
+/* ---- library information (info.h:7-8) ----------------------------------------------------- */
+const char *ts_version(void);
+/* Copies the JSON report (NUL-terminated) into buf when it fits; *needed gets its size + 1. */
+int ts_info_json(char *buf, uint64_t capacity, uint64_t *needed);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TILESTREAM_C_H */

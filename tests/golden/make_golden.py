@@ -1,0 +1,93 @@
+"""Regenerates the golden .tsc fixtures of this directory with the reference's own encoder.
+
+The eight single-tile cases are the hand-calculated golden inputs of the reference tests
+(tests/cpu_codec_test.cpp:86-104 for uint16, tests/fp32_codec_test.cpp:81-82 for float32). Each
+input is encoded by the reference CPU codec compiled from its sources (oracle/_ref, built by
+oracle/Makefile) and written as a .hex file in the reference's text layout. When the reference
+checkout is present the script also asserts that every regenerated file equals the reference's
+own golden file byte for byte.
+
+It also records the C1 golden round trip (uint16 1024x1024 frame, seed 1, tiles 128x32): the
+SHA-256 and size of the reference encoding, in c1_roundtrip.json.
+
+Run from the repository root:  python tests/golden/make_golden.py
+"""
+import hashlib
+import json
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+import oracle  # noqa: E402
+from tilestream_b200 import workloads  # noqa: E402
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def cases():
+    zero_width = [0x0102] * 8 + [0x0304] * 8
+    half_range = [0, 32768, 0, 32768, 0, 32768, 0, 32768, 0] + [5] * 9
+    u16 = np.uint16
+    return [
+        ("uint16_raw", 1, 1, np.array([0x1234], u16), oracle.RAW),
+        ("uint16_constant", 3, 2, np.full(6, 0xbeef, u16), oracle.CONSTANT),
+        ("uint16_wrap", 8, 2, np.array([65535, 0, 1, 2, 3, 4, 5, 6, 0, 65535, 65534, 65533,
+                                        65532, 65531, 65530, 65529], u16), oracle.PREDICT),
+        ("uint16_zero_width", 8, 2, np.array(zero_width, u16), oracle.PREDICT),
+        ("uint16_raw_tie", 6, 1, np.arange(6, dtype=u16), oracle.RAW),
+        ("uint16_half_range", 9, 2, np.array(half_range, u16), oracle.PREDICT),
+        ("float32_raw", 1, 1, np.array([0x7fc01234], np.uint32), oracle.RAW),
+        ("float32_negative_zero_constant", 3, 2, np.full(6, 0x80000000, np.uint32),
+         oracle.CONSTANT),
+    ]
+
+
+def to_hex(data: bytes) -> str:
+    """Eight bytes per line for the 64-byte header and each 32-byte index entry, then the
+    payload, as in the reference's golden files."""
+    lines = [" ".join(f"{b:02x}" for b in data[i:i + 8]) for i in range(0, len(data), 8)]
+    return "\n".join(lines) + "\n"
+
+
+def read_hex(path: str) -> bytes:
+    with open(path) as f:
+        return bytes(int(tok, 16) for tok in f.read().split())
+
+
+def main():
+    ref = oracle.Reference()
+    manifest = {}
+    for name, w, h, pixels, mode in cases():
+        ptype = oracle.UINT16 if pixels.dtype == np.uint16 else oracle.FLOAT32
+        data = ref.compress(pixels, ptype, w, h, w * oracle.SAMPLE[ptype])
+        path = os.path.join(HERE, name + ".hex")
+        with open(path, "w") as f:
+            f.write(to_hex(data))
+        manifest[name] = {"width": w, "height": h, "type": ptype, "mode": mode,
+                          "pixels": [int(v) for v in pixels]}
+        upstream = os.path.join(oracle.REFERENCE_DIR, "tests", "golden", name + ".hex")
+        if os.path.exists(upstream):
+            assert read_hex(upstream) == data, f"{name}: differs from the reference golden file"
+    with open(os.path.join(HERE, "cases.json"), "w") as f:
+        json.dump(manifest, f, indent=1)
+        f.write("\n")
+
+    frame = workloads.detector_frame(1024, 1024, seed=1)
+    data = ref.compress_image(frame, (128, 32))
+    st, back = ref.decompress(data, oracle.UINT16, 1024, 1024)
+    assert st == 0 and np.array_equal(back.view(np.uint16).reshape(1024, 1024), frame)
+    with open(os.path.join(HERE, "c1_roundtrip.json"), "w") as f:
+        json.dump({"config": "uint16 1024x1024 detector frame, seed 1, tiles 128x32",
+                   "pixels_sha256": hashlib.sha256(frame.tobytes()).hexdigest(),
+                   "file_bytes": len(data),
+                   "file_sha256": hashlib.sha256(data).hexdigest()}, f, indent=1)
+        f.write("\n")
+    print("golden fixtures written")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,281 @@
+// The C entry layer of include/tilestream_c.h over the C++ API.
+#include <tilestream/cpu.h>
+#include <tilestream/cuda.h>
+#include <tilestream/info.h>
+#include <tilestream_c.h>
+
+#include "plan.h"
+
+#include <cstddef>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+namespace ts = tilestream;
+
+// Each C record has the layout of the C++ record it mirrors.
+#define TS_SAME_LAYOUT(C, CPP)                                                                    \
+    static_assert(sizeof(C) == sizeof(CPP) && alignof(C) == alignof(CPP), #C " layout")
+TS_SAME_LAYOUT(ts_image_spec, ts::ImageSpec);
+TS_SAME_LAYOUT(ts_tile_shape, ts::TileShape);
+TS_SAME_LAYOUT(ts_roi, ts::Roi);
+TS_SAME_LAYOUT(ts_const_bytes, ts::ConstBytes);
+TS_SAME_LAYOUT(ts_mutable_bytes, ts::MutableBytes);
+TS_SAME_LAYOUT(ts_const_image_view, ts::ConstImageView);
+TS_SAME_LAYOUT(ts_image_view, ts::ImageView);
+TS_SAME_LAYOUT(ts_device_result, ts::DeviceResult);
+TS_SAME_LAYOUT(ts_parameter, ts::cuda::Parameter);
+TS_SAME_LAYOUT(ts_calibration, ts::cuda::Calibration);
+TS_SAME_LAYOUT(ts_tile_mapping, ts::cuda::TileMapping);
+TS_SAME_LAYOUT(ts_parse_limits, ts::ParseLimits);
+TS_SAME_LAYOUT(ts_workspace_spec, ts::WorkspaceSpec);
+TS_SAME_LAYOUT(ts_tile_metadata, ts::TileMetadata);
+TS_SAME_LAYOUT(ts_segment_metadata, ts::SegmentMetadata);
+TS_SAME_LAYOUT(ts_compressed_input, ts::cuda::CompressedInput);
+TS_SAME_LAYOUT(ts_batch_item, ts::cuda::BatchItem);
+TS_SAME_LAYOUT(ts_batch_request, ts::cuda::BatchRequest);
+TS_SAME_LAYOUT(ts_result_buffer, ts::cuda::ResultBuffer);
+static_assert(offsetof(ts_batch_item, compressed_input) ==
+              offsetof(ts::cuda::BatchItem, compressed_input));
+static_assert(offsetof(ts_batch_item, calibration) == offsetof(ts::cuda::BatchItem, calibration));
+static_assert(offsetof(ts_compressed_input, metadata) ==
+              offsetof(ts::cuda::CompressedInput, metadata));
+static_assert(offsetof(ts_compressed_input, trusted_tile) ==
+              offsetof(ts::cuda::CompressedInput, trusted_tile));
+static_assert(sizeof(ts::cuda::DeviceTile) == 40 && sizeof(ts::cuda::DeviceSegment) == 16 &&
+              sizeof(ts::DeviceResult) == 16);
+static_assert(std::is_trivially_copyable_v<ts::cuda::DeviceImage> &&
+              std::is_standard_layout_v<ts::cuda::DeviceBatch>);
+
+struct ts_metadata {
+    ts::ImageMetadata value;
+};
+
+struct ts_plan {
+    std::unique_ptr<ts::cuda::BatchPlan> plan;
+};
+
+namespace {
+
+template <typename To, typename From> To as(const From &from) {
+    static_assert(sizeof(To) == sizeof(From));
+    To to;
+    std::memcpy(static_cast<void *>(&to), &from, sizeof(To));
+    return to;
+}
+
+int code(ts::Status s) {
+    return static_cast<int>(s);
+}
+
+cudaStream_t stream_of(void *s) {
+    return static_cast<cudaStream_t>(s);
+}
+
+ts::ParseLimits limits_of(const ts_parse_limits *l) {
+    return l != nullptr ? as<ts::ParseLimits>(*l) : ts::ParseLimits{};
+}
+
+} // namespace
+
+extern "C" {
+
+int ts_image_span(ts_image_spec image, uint64_t pitch_bytes, uint64_t *bytes) {
+    return code(ts::image_span(as<ts::ImageSpec>(image), pitch_bytes, *bytes));
+}
+
+int ts_compress_bound(ts_image_spec image, ts_tile_shape tile, uint64_t *bytes) {
+    return code(ts::compress_bound(as<ts::ImageSpec>(image), as<ts::TileShape>(tile), *bytes));
+}
+
+int ts_workspace_size(const ts_workspace_spec *spec, uint64_t *bytes) {
+    return code(ts::workspace_size(as<ts::WorkspaceSpec>(*spec), *bytes));
+}
+
+int ts_parse_metadata(ts_const_bytes source, const ts_parse_limits *limits, ts_metadata **out) {
+    std::unique_ptr<ts_metadata> m(new (std::nothrow) ts_metadata);
+    if (!m) {
+        return code(ts::Status::resource_limit);
+    }
+    const ts::Status st =
+        ts::parse_metadata(as<ts::ConstBytes>(source), limits_of(limits), m->value);
+    if (st == ts::Status::success) {
+        *out = m.release();
+    }
+    return code(st);
+}
+
+int ts_metadata_create(ts_image_spec image, ts_tile_shape tile, uint64_t file_bytes,
+                       const ts_tile_metadata *tiles, uint64_t tile_count,
+                       const ts_segment_metadata *segments, uint64_t segment_count,
+                       ts_metadata **out) {
+    if ((tiles == nullptr && tile_count != 0) || (segments == nullptr && segment_count != 0)) {
+        return code(ts::Status::invalid_argument);
+    }
+    try {
+        auto m = std::make_unique<ts_metadata>();
+        m->value.image = as<ts::ImageSpec>(image);
+        m->value.tile = as<ts::TileShape>(tile);
+        m->value.file_bytes = file_bytes;
+        m->value.tiles.resize(tile_count);
+        m->value.segments.resize(segment_count);
+        if (tile_count != 0) {
+            std::memcpy(static_cast<void *>(m->value.tiles.data()), tiles,
+                        tile_count * sizeof(ts_tile_metadata));
+        }
+        if (segment_count != 0) {
+            std::memcpy(static_cast<void *>(m->value.segments.data()), segments,
+                        segment_count * sizeof(ts_segment_metadata));
+        }
+        *out = m.release();
+        return code(ts::Status::success);
+    } catch (...) {
+        return code(ts::Status::resource_limit);
+    }
+}
+
+void ts_metadata_destroy(ts_metadata *metadata) {
+    delete metadata;
+}
+
+void ts_metadata_info(const ts_metadata *m, ts_image_spec *image, ts_tile_shape *tile,
+                      uint64_t *file_bytes, uint64_t *tile_count, uint64_t *segment_count) {
+    if (image) *image = as<ts_image_spec>(m->value.image);
+    if (tile) *tile = as<ts_tile_shape>(m->value.tile);
+    if (file_bytes) *file_bytes = m->value.file_bytes;
+    if (tile_count) *tile_count = m->value.tiles.size();
+    if (segment_count) *segment_count = m->value.segments.size();
+}
+
+const ts_tile_metadata *ts_metadata_tiles(const ts_metadata *m) {
+    return reinterpret_cast<const ts_tile_metadata *>(m->value.tiles.data());
+}
+
+const ts_segment_metadata *ts_metadata_segments(const ts_metadata *m) {
+    return reinterpret_cast<const ts_segment_metadata *>(m->value.segments.data());
+}
+
+int ts_cpu_compress(ts_const_image_view input, ts_tile_shape tile, ts_mutable_bytes output,
+                    uint64_t *bytes_written) {
+    return code(ts::cpu::compress(as<ts::ConstImageView>(input), as<ts::TileShape>(tile),
+                                  as<ts::MutableBytes>(output), *bytes_written));
+}
+
+int ts_cpu_decompress(ts_const_bytes input, ts_image_view output, const ts_parse_limits *limits) {
+    return code(ts::cpu::decompress(as<ts::ConstBytes>(input), as<ts::ImageView>(output),
+                                    limits_of(limits)));
+}
+
+int ts_prepare_batch(const ts_batch_request *request, ts_plan **plan, void *stream) {
+    if (request == nullptr || plan == nullptr) {
+        return code(ts::Status::invalid_argument);
+    }
+    try {
+        ts::cuda::BatchRequest r = as<ts::cuda::BatchRequest>(*request);
+        std::vector<ts::cuda::BatchItem> items;
+        if (request->items != nullptr && request->count <= UINT32_MAX) {
+            items.resize(request->count);
+            for (uint64_t i = 0; i < request->count; ++i) {
+                items[i] = as<ts::cuda::BatchItem>(request->items[i]);
+                const ts_metadata *m = request->items[i].compressed_input.metadata;
+                items[i].compressed_input.metadata = m != nullptr ? &m->value : nullptr;
+            }
+            r.items = items.data();
+        }
+        auto holder = std::make_unique<ts_plan>();
+        const ts::Status st = ts::cuda::prepare_batch(r, holder->plan, stream_of(stream));
+        if (st == ts::Status::success) {
+            delete *plan;
+            *plan = holder.release();
+        }
+        return code(st);
+    } catch (...) {
+        return code(ts::Status::resource_limit);
+    }
+}
+
+void ts_plan_destroy(ts_plan *plan) {
+    delete plan;
+}
+
+int ts_plan_workspace_spec(const ts_plan *plan, ts_workspace_spec *spec) {
+    if (plan == nullptr || !plan->plan || spec == nullptr) {
+        return code(ts::Status::invalid_argument);
+    }
+    *spec = as<ts_workspace_spec>(plan->plan->workspace_spec());
+    return 0;
+}
+
+#define TS_EXECUTOR(name)                                                                         \
+    int ts_##name(const ts_plan *plan, ts_mutable_bytes workspace, ts_result_buffer results,      \
+                  void *stream) {                                                                 \
+        if (plan == nullptr || !plan->plan) {                                                     \
+            return code(ts::Status::invalid_argument);                                            \
+        }                                                                                         \
+        return code(ts::cuda::name(*plan->plan, as<ts::MutableBytes>(workspace),                  \
+                                   as<ts::cuda::ResultBuffer>(results), stream_of(stream)));      \
+    }
+TS_EXECUTOR(compress_async)
+TS_EXECUTOR(decompress_async)
+TS_EXECUTOR(decode_roi_async)
+TS_EXECUTOR(calibrate_async)
+TS_EXECUTOR(decode_calibrate_async)
+#undef TS_EXECUTOR
+
+// Same contract as DeviceBuffer::allocate (cuda.h:124-125); the caller owns the memory and frees
+// it with ts_device_release.
+int ts_device_allocate(uint64_t bytes, void *stream, void **data) {
+    if (bytes > ts::max_bytes) {
+        return code(ts::Status::size_overflow);
+    }
+    if (bytes == 0) {
+        *data = nullptr;
+        return 0;
+    }
+    void *p = nullptr;
+    if (cudaMallocAsync(&p, static_cast<std::size_t>(bytes), stream_of(stream)) != cudaSuccess) {
+        return code(ts::cuda::detail::cuda_failure());
+    }
+    if (reinterpret_cast<std::uintptr_t>(p) % ts::workspace_alignment != 0) {
+        static_cast<void>(cudaFreeAsync(p, stream_of(stream)));
+        return code(ts::Status::cuda_error);
+    }
+    *data = p;
+    return 0;
+}
+
+int ts_device_release(void *data, void *stream) {
+    if (data == nullptr) {
+        return 0;
+    }
+    return code(ts::cuda::detail::cuda_status(cudaFreeAsync(data, stream_of(stream))));
+}
+
+int ts_synchronize(void *stream) {
+    return code(ts::cuda::synchronize(stream_of(stream)));
+}
+
+const char *ts_version(void) {
+    return ts::version();
+}
+
+int ts_info_json(char *buf, uint64_t capacity, uint64_t *needed) {
+    try {
+        const std::string s = ts::info_json();
+        if (needed != nullptr) {
+            *needed = s.size() + 1;
+        }
+        if (buf != nullptr && capacity >= s.size() + 1) {
+            std::memcpy(buf, s.c_str(), s.size() + 1);
+            return 0;
+        }
+        return code(ts::Status::buffer_too_small);
+    } catch (...) {
+        return code(ts::Status::resource_limit);
+    }
+}
+
+} // extern "C"

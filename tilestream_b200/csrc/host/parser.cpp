@@ -1,0 +1,237 @@
+// Untrusted .tsc parser (include/tilestream/api.h; reference: src/cpu/parser.cpp:27-242).
+//
+// Validation order and status mapping follow docs/format.md:136-147 and docs/api.md:43-47:
+// the fixed header first, then the caller's budgets, then every index entry, payload and row
+// descriptor (lengths before contents, widths before arithmetic), then the native tables are
+// allocated and filled. The budget counts native table bytes; sizeof values below are those of
+// the public records. On failure the caller's metadata is untouched.
+#include <tilestream/api.h>
+
+#include "checked.h"
+
+#include <algorithm>
+#include <new>
+#include <stdexcept>
+#include <utility>
+
+namespace tilestream {
+namespace {
+
+using host::le;
+using host::zeros;
+
+struct Header {
+    ImageSpec image;
+    TileShape tile;
+    std::uint64_t across = 0;
+    std::uint64_t count = 0;
+    std::uint64_t payload = 0;
+};
+
+Status read_header(const std::uint8_t *d, std::uint64_t size, Header &h) noexcept {
+    if (size < format::header_bytes) {
+        return Status::malformed_data;
+    }
+    for (std::size_t i = 0; i < format::magic.size(); ++i) {
+        if (d[i] != format::magic[i]) {
+            return Status::malformed_data;
+        }
+    }
+    if (le(d + format::header::version_major, 2) != format::major_version ||
+        le(d + format::header::version_minor, 2) != format::minor_version ||
+        d[format::header::flags] != 0) {
+        return Status::unsupported_format;
+    }
+    if (le(d + format::header::size, 2) != format::header_bytes ||
+        le(d + format::header::entry_size, 2) != format::index_entry_bytes ||
+        !zeros(d + format::header::reserved, 2)) {
+        return Status::malformed_data;
+    }
+    const std::uint8_t type = d[format::header::pixel_type];
+    if (type != static_cast<std::uint8_t>(PixelType::uint16) &&
+        type != static_cast<std::uint8_t>(PixelType::float32)) {
+        return Status::unsupported_type;
+    }
+    h.image = {static_cast<PixelType>(type),
+               static_cast<std::uint32_t>(le(d + format::header::width, 4)),
+               static_cast<std::uint32_t>(le(d + format::header::height, 4))};
+    h.tile = {static_cast<std::uint16_t>(le(d + format::header::tile_width, 2)),
+              static_cast<std::uint16_t>(le(d + format::header::tile_height, 2))};
+    if (h.image.width == 0 || h.image.height == 0) {
+        return Status::malformed_data;
+    }
+    if (!host::supported_tile(h.tile)) {
+        return Status::unsupported_format;
+    }
+    std::uint64_t bound = 0;
+    const Status st = compress_bound(h.image, h.tile, bound);
+    if (st != Status::success) {
+        return st;
+    }
+    h.across = host::ceil_div(h.image.width, h.tile.width);
+    const std::uint64_t down = host::ceil_div(h.image.height, h.tile.height);
+    std::uint64_t index = 0;
+    if (!host::mul(h.across, down, h.count) ||
+        !host::mul(h.count, format::index_entry_bytes, index) ||
+        !host::add(format::header_bytes, index, h.payload)) {
+        return Status::size_overflow;
+    }
+    if (le(d + format::header::tile_count, 8) != h.count ||
+        le(d + format::header::index_offset, 8) != format::header_bytes ||
+        le(d + format::header::payload_offset, 8) != h.payload ||
+        le(d + format::header::file_size, 8) != size || size > bound || h.payload > size) {
+        return Status::malformed_data;
+    }
+    return Status::success;
+}
+
+// Validates every tile. With out == nullptr only the row segments are counted.
+Status walk(const std::uint8_t *d, std::uint64_t size, const Header &h, std::uint64_t &segments,
+            ImageMetadata *out) noexcept {
+    const std::uint64_t s = h.image.type == PixelType::uint16 ? 2 : 4;
+    const std::uint32_t max_bits = h.image.type == PixelType::uint16 ? 16 : 32;
+    std::uint64_t expected = h.payload;
+    std::uint64_t nseg = 0;
+    for (std::uint64_t i = 0; i < h.count; ++i) {
+        const std::uint8_t *e = d + format::header_bytes + i * format::index_entry_bytes;
+        const std::uint64_t x = (i % h.across) * h.tile.width;
+        const std::uint64_t y = (i / h.across) * h.tile.height;
+        const std::uint64_t w = std::min<std::uint64_t>(h.tile.width, h.image.width - x);
+        const std::uint64_t ht = std::min<std::uint64_t>(h.tile.height, h.image.height - y);
+        const std::uint64_t offset = le(e + format::entry::offset, 8);
+        const std::uint64_t length = le(e + format::entry::length, 8);
+        const std::uint64_t raw = w * ht * s;
+        const std::uint64_t raw4 = (raw + 3) / 4 * 4;
+        const std::uint8_t mode = e[format::entry::mode];
+        if (mode > static_cast<std::uint8_t>(TileMode::predict_bitpack) ||
+            !zeros(e + format::entry::reserved, 3) || !zeros(e + format::entry::reserved_tail, 8) ||
+            le(e + format::entry::width, 2) != w || le(e + format::entry::height, 2) != ht ||
+            offset != expected || offset > size || length > size - offset || length == 0 ||
+            length % 4 != 0 || length > raw4) {
+            return Status::malformed_data;
+        }
+        const std::uint8_t *p = d + offset;
+        const std::uint64_t first = mode == 2 ? nseg : 0;
+        if (mode == 0) {
+            if (length != raw4 || !zeros(p + raw, length - raw)) {
+                return Status::malformed_data;
+            }
+        } else if (mode == 1) {
+            if (length != 4 || (s == 2 && !zeros(p + 2, 2))) {
+                return Status::malformed_data;
+            }
+        } else {
+            std::uint64_t cursor = 0;
+            for (std::uint64_t r = 0; r < ht; ++r) {
+                if (length - cursor < format::segment_header_bytes) {
+                    return Status::malformed_data;
+                }
+                const std::uint8_t *desc = p + cursor;
+                const auto seed = static_cast<std::uint32_t>(le(desc + format::segment::seed, 4));
+                const std::uint32_t bits = desc[format::segment::bit_width];
+                if ((s == 2 && seed > UINT16_MAX) || bits > max_bits || (w == 1 && bits != 0) ||
+                    !zeros(desc + format::segment::reserved, 3)) {
+                    return Status::malformed_data;
+                }
+                cursor += format::segment_header_bytes;
+                const std::uint64_t nbits = (w - 1) * bits;
+                const std::uint64_t packed = (nbits + 31) / 32 * 4;
+                if (packed > length - cursor) {
+                    return Status::malformed_data;
+                }
+                // Unused high bits of the last word must be zero.
+                if (nbits % 32 != 0 && (le(p + cursor + packed - 4, 4) >> (nbits % 32)) != 0) {
+                    return Status::malformed_data;
+                }
+                if (out != nullptr) {
+                    out->segments[nseg] = {seed, bits, cursor, packed};
+                }
+                ++nseg;
+                cursor += packed;
+            }
+            if (cursor != length) {
+                return Status::malformed_data;
+            }
+        }
+        if (out != nullptr) {
+            out->tiles[i] = {static_cast<TileMode>(mode), static_cast<std::uint16_t>(w),
+                             static_cast<std::uint16_t>(ht), offset, length, first};
+        }
+        expected += length;
+    }
+    segments = nseg;
+    return expected == size ? Status::success : Status::malformed_data;
+}
+
+Status table_bytes(std::uint64_t tiles, std::uint64_t segments, std::uint64_t &bytes) noexcept {
+    std::uint64_t t = 0, g = 0, total = 0;
+    if (!host::mul(tiles, sizeof(TileMetadata), t) ||
+        !host::mul(segments, sizeof(SegmentMetadata), g) ||
+        !host::add(sizeof(ImageMetadata), t, total) || !host::add(total, g, total)) {
+        return Status::size_overflow;
+    }
+    bytes = total;
+    return Status::success;
+}
+
+} // namespace
+
+Status parse_metadata(ConstBytes source, const ParseLimits &limits,
+                      ImageMetadata &metadata) noexcept {
+    Status st = host::byte_range(source.data, source.size);
+    if (st != Status::success) {
+        return st;
+    }
+    if (source.size > limits.file_bytes) {
+        return Status::resource_limit;
+    }
+    const auto *d = static_cast<const std::uint8_t *>(source.data);
+    Header h;
+    st = read_header(d, source.size, h);
+    if (st != Status::success) {
+        return st;
+    }
+    if (h.count > limits.tile_count) {
+        return Status::resource_limit;
+    }
+    std::uint64_t need = 0;
+    st = table_bytes(h.count, 0, need);
+    if (st != Status::success) {
+        return st;
+    }
+    if (need > limits.metadata_bytes) {
+        return Status::resource_limit;
+    }
+    std::uint64_t segments = 0;
+    st = walk(d, source.size, h, segments, nullptr);
+    if (st != Status::success) {
+        return st;
+    }
+    st = table_bytes(h.count, segments, need);
+    if (st != Status::success) {
+        return st;
+    }
+    if (need > limits.metadata_bytes) {
+        return Status::resource_limit;
+    }
+    try {
+        ImageMetadata parsed;
+        parsed.image = h.image;
+        parsed.tile = h.tile;
+        parsed.file_bytes = source.size;
+        parsed.tiles.resize(static_cast<std::size_t>(h.count));
+        parsed.segments.resize(static_cast<std::size_t>(segments));
+        st = walk(d, source.size, h, segments, &parsed);
+        if (st != Status::success) {
+            return st;
+        }
+        metadata = std::move(parsed);
+        return Status::success;
+    } catch (const std::bad_alloc &) {
+        return Status::resource_limit;
+    } catch (const std::length_error &) {
+        return Status::resource_limit;
+    }
+}
+
+} // namespace tilestream

@@ -1,0 +1,828 @@
+// prepare_batch, check_execution and the five executors of include/tilestream/cuda.h.
+//
+// Host validation covers the same conditions, in the same order and with the same statuses, as
+// the reference planner (src/cuda/plan.cpp:128-465, 627-711), so error behaviour is a drop-in.
+// What the plan builds is different: instead of DeviceImage/DeviceTile/DeviceSegment tables
+// split into 4096-tile windows with a binary search per block, every execution is one
+// persistent launch over a flat queue of self-contained tasks (tsk_decode_task, one per tile
+// to decode, 48 bytes), plus a 16-byte-aligned slot of row starts per predictive tile that the
+// kernel stages with the payload. The WorkspaceSpec reported to callers is still the
+// reference's per-window bound, so workspace_size() callers allocate what they always did.
+#include "plan.h"
+
+#include <algorithm>
+#include <cstring>
+#include <new>
+#include <stdexcept>
+#include <utility>
+
+namespace tilestream::cuda {
+namespace detail {
+
+constexpr std::uint32_t kWindowTiles = 4096; // the reference's window bound (plan.h:14)
+
+bool RangeSet::assign(std::vector<Range> writable, std::vector<Range> readable) {
+    auto empty = [](const Range &r) { return r.begin == r.end; };
+    auto by_begin = [](const Range &a, const Range &b) { return a.begin < b.begin; };
+    writable.erase(std::remove_if(writable.begin(), writable.end(), empty), writable.end());
+    readable.erase(std::remove_if(readable.begin(), readable.end(), empty), readable.end());
+    std::sort(writable.begin(), writable.end(), by_begin);
+    std::sort(readable.begin(), readable.end(), by_begin);
+    for (std::size_t i = 1; i < writable.size(); ++i) {
+        if (writable[i].begin < writable[i - 1].end) {
+            return false;
+        }
+    }
+    std::vector<std::uintptr_t> max_end(readable.size());
+    std::uintptr_t reach = 0;
+    for (std::size_t i = 0; i < readable.size(); ++i) {
+        reach = std::max(reach, readable[i].end);
+        max_end[i] = reach;
+    }
+    readable_ = std::move(readable);
+    max_end_ = std::move(max_end);
+    writable_.clear();
+    for (const Range &r : writable) {
+        if (!disjoint(r)) {
+            return false;
+        }
+    }
+    writable_ = std::move(writable);
+    return true;
+}
+
+bool RangeSet::disjoint(Range range) const noexcept {
+    if (range.begin == range.end) {
+        return true;
+    }
+    auto starts_before = [](const Range &r, std::uintptr_t end) { return r.begin < end; };
+    // Writable ranges are disjoint and sorted: only the last one starting before range.end can
+    // reach into it.
+    auto w = std::lower_bound(writable_.begin(), writable_.end(), range.end, starts_before);
+    if (w != writable_.begin() && std::prev(w)->end > range.begin) {
+        return false;
+    }
+    auto r = std::lower_bound(readable_.begin(), readable_.end(), range.end, starts_before);
+    const auto n = static_cast<std::size_t>(r - readable_.begin());
+    return n == 0 || max_end_[n - 1] <= range.begin;
+}
+
+PlanState::~PlanState() {
+    // Executions must have finished (docs/api.md:71), so the free needs no ordering.
+    if (storage != nullptr) {
+        static_cast<void>(cuda_status(cudaFreeAsync(storage, cudaStreamPerThread)));
+    }
+}
+
+Status accessible(const void *data, int device, bool pageable) noexcept {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, data) != cudaSuccess) {
+        return cuda_failure();
+    }
+    switch (a.type) {
+    case cudaMemoryTypeDevice:
+        return a.device == device ? Status::success : Status::invalid_argument;
+    case cudaMemoryTypeManaged:
+        return Status::success;
+    case cudaMemoryTypeHost:
+        return a.devicePointer == data ? Status::success : Status::invalid_argument;
+    default:
+        return pageable ? Status::success : Status::invalid_argument;
+    }
+}
+
+Status stream_device(cudaStream_t stream, int device) noexcept {
+    int current = 0, owner = 0;
+    if (cudaGetDevice(&current) != cudaSuccess || cudaStreamGetDevice(stream, &owner) != cudaSuccess) {
+        return cuda_failure();
+    }
+    return current == device && owner == device ? Status::success : Status::invalid_argument;
+}
+
+namespace {
+
+std::uint64_t tiles_across(const ImageSpec &im, TileShape t) noexcept {
+    return host::ceil_div(im.width, t.width);
+}
+std::uint64_t tiles_down(const ImageSpec &im, TileShape t) noexcept {
+    return host::ceil_div(im.height, t.height);
+}
+
+// Host-side draft of a plan: validated descriptors and the ranges/pointers to check.
+struct Draft {
+    PixelType type = PixelType::uint16;
+    TileShape shape;
+    std::vector<std::uint64_t> tiles_per_image; // for the reference window accounting
+    std::vector<Range> writable, readable;
+    std::vector<const void *> pointers;
+
+    std::vector<tsk_decode_image> images;
+    std::vector<tsk_decode_task> tasks;
+    std::vector<tsk_row_start> rows;
+    bool trusted = false;
+
+    std::vector<tsk_encode_image> encode_images;
+    std::uint64_t total_tiles = 0;
+
+    std::vector<tsk_calib_image> calib_images;
+    std::vector<tsk_calib_task> calib_tasks;
+};
+
+Status draft_compress(const BatchRequest &request, Draft &d) {
+    d.type = request.items[0].input.image.type;
+    d.shape = request.tile;
+    for (std::uint64_t i = 0; i < request.count; ++i) {
+        const BatchItem &item = request.items[i];
+        Status st = host::view_ok(item.input);
+        if (st != Status::success) {
+            return st;
+        }
+        if (item.input.image.type != d.type) {
+            return Status::invalid_argument;
+        }
+        std::uint64_t bound = 0;
+        st = compress_bound(item.input.image, request.tile, bound);
+        if (st != Status::success) {
+            return st;
+        }
+        const MutableBytes &out = item.compressed_output;
+        st = host::byte_range(out.data, out.size);
+        if (st != Status::success) {
+            return st;
+        }
+        if (out.data == nullptr || reinterpret_cast<std::uintptr_t>(out.data) % 4 != 0) {
+            return Status::invalid_argument;
+        }
+        if (out.size < bound) {
+            return Status::buffer_too_small;
+        }
+        tsk_encode_image e{};
+        e.input = reinterpret_cast<std::uint64_t>(item.input.data);
+        e.pitch = item.input.pitch_bytes;
+        e.output = reinterpret_cast<std::uint64_t>(out.data);
+        e.columns = tiles_across(item.input.image, request.tile);
+        e.tile_count = e.columns * tiles_down(item.input.image, request.tile);
+        e.first_tile = d.total_tiles;
+        e.width = item.input.image.width;
+        e.height = item.input.image.height;
+        e.tile_width = request.tile.width;
+        e.tile_height = request.tile.height;
+        e.type = static_cast<std::uint32_t>(item.input.image.type);
+        d.total_tiles += e.tile_count;
+        d.encode_images.push_back(e);
+        d.tiles_per_image.push_back(e.tile_count);
+        d.readable.push_back(range_of(item.input.data, item.input.capacity_bytes));
+        d.writable.push_back(range_of(out.data, out.size));
+        d.pointers.push_back(item.input.data);
+        d.pointers.push_back(out.data);
+    }
+    return Status::success;
+}
+
+// A map matches the output region exactly and is addressed in output coordinates.
+Status check_parameter(const Parameter &p, const ImageSpec &region, Draft &d) {
+    if (p.kind == ParameterKind::scalar) {
+        return Status::success;
+    }
+    if (p.kind != ParameterKind::map) {
+        return Status::invalid_argument;
+    }
+    const Status st = host::view_ok(p.map);
+    if (st != Status::success) {
+        return st;
+    }
+    if (p.map.image.type != PixelType::float32 || p.map.image.width != region.width ||
+        p.map.image.height != region.height) {
+        return Status::invalid_argument;
+    }
+    d.readable.push_back(range_of(p.map.data, p.map.capacity_bytes));
+    d.pointers.push_back(p.map.data);
+    return Status::success;
+}
+
+Status check_calibration(const Calibration &c, const ImageSpec &region, Draft &d) {
+    const Status st = check_parameter(c.offset, region, d);
+    return st != Status::success ? st : check_parameter(c.gain, region, d);
+}
+
+void set_parameters(const Calibration &c, std::uint64_t &offset_map, std::uint64_t &offset_pitch,
+                    float &offset, std::uint64_t &gain_map, std::uint64_t &gain_pitch,
+                    float &gain) {
+    offset_map = c.offset.kind == ParameterKind::map
+                     ? reinterpret_cast<std::uint64_t>(c.offset.map.data)
+                     : 0;
+    offset_pitch = c.offset.map.pitch_bytes;
+    offset = c.offset.scalar;
+    gain_map =
+        c.gain.kind == ParameterKind::map ? reinterpret_cast<std::uint64_t>(c.gain.map.data) : 0;
+    gain_pitch = c.gain.map.pitch_bytes;
+    gain = c.gain.scalar;
+}
+
+Status draft_calibrate(const BatchRequest &request, Draft &d) {
+    d.type = request.items[0].input.image.type;
+    for (std::uint64_t i = 0; i < request.count; ++i) {
+        const BatchItem &item = request.items[i];
+        Status st = host::view_ok(item.input);
+        if (st == Status::success) {
+            st = host::view_ok(item.output);
+        }
+        if (st != Status::success) {
+            return st;
+        }
+        if (item.input.image.type != d.type || item.output.image.type != PixelType::float32 ||
+            item.output.image.width != item.input.image.width ||
+            item.output.image.height != item.input.image.height) {
+            return Status::invalid_argument;
+        }
+        st = check_calibration(item.calibration, item.output.image, d);
+        if (st != Status::success) {
+            return st;
+        }
+        tsk_calib_image c{};
+        c.input = reinterpret_cast<std::uint64_t>(item.input.data);
+        c.in_pitch = item.input.pitch_bytes;
+        c.out = reinterpret_cast<std::uint64_t>(item.output.data);
+        c.out_pitch = item.output.pitch_bytes;
+        set_parameters(item.calibration, c.offset_map, c.offset_pitch, c.offset, c.gain_map,
+                       c.gain_pitch, c.gain);
+        c.width = item.input.image.width;
+        c.height = item.input.image.height;
+        c.type = static_cast<std::uint32_t>(item.input.image.type);
+        const auto image = static_cast<std::uint32_t>(d.calib_images.size());
+        // Chunks of about 16 Ki pixels keep every SM streaming on small and large images alike.
+        const std::uint32_t chunk = std::max<std::uint32_t>(1, 16384 / c.width);
+        for (std::uint32_t y = 0; y < c.height; y += chunk) {
+            tsk_calib_task t{};
+            t.image = image;
+            t.y0 = y;
+            t.rows = std::min(chunk, c.height - y);
+            t.reserved = y == 0 ? 1u : 0u; // first chunk writes the result record
+            d.calib_tasks.push_back(t);
+        }
+        d.calib_images.push_back(c);
+        d.tiles_per_image.push_back(0);
+        d.readable.push_back(range_of(item.input.data, item.input.capacity_bytes));
+        d.writable.push_back(range_of(item.output.data, item.output.capacity_bytes));
+        d.pointers.push_back(item.input.data);
+        d.pointers.push_back(item.output.data);
+    }
+    return Status::success;
+}
+
+// Repeats the parser's structural checks that keep device reads inside the tile payload
+// (reference plan.cpp:237-279).
+Status check_tile(const ImageMetadata &m, std::uint64_t index) noexcept {
+    const TileMetadata &t = m.tiles[static_cast<std::size_t>(index)];
+    const std::uint64_t across = tiles_across(m.image, m.tile);
+    const std::uint64_t x = index % across * m.tile.width;
+    const std::uint64_t y = index / across * m.tile.height;
+    const std::uint64_t w = std::min<std::uint64_t>(m.tile.width, m.image.width - x);
+    const std::uint64_t h = std::min<std::uint64_t>(m.tile.height, m.image.height - y);
+    const std::uint64_t s = m.image.type == PixelType::uint16 ? 2 : 4;
+    const std::uint32_t max_bits = m.image.type == PixelType::uint16 ? 16 : 32;
+    const std::uint64_t raw = (w * h * s + 3) / 4 * 4;
+    if (t.width != w || t.height != h || t.offset % 4 != 0 || t.offset > m.file_bytes ||
+        t.length > m.file_bytes - t.offset) {
+        return Status::malformed_data;
+    }
+    switch (t.mode) {
+    case TileMode::raw:
+        return t.length == raw ? Status::success : Status::malformed_data;
+    case TileMode::constant:
+        return t.length == 4 ? Status::success : Status::malformed_data;
+    case TileMode::predict_bitpack:
+        break;
+    default:
+        return Status::malformed_data;
+    }
+    if (t.length > raw || t.first_segment > m.segments.size() ||
+        h > m.segments.size() - t.first_segment) {
+        return Status::malformed_data;
+    }
+    for (std::uint64_t r = 0; r < h; ++r) {
+        const SegmentMetadata &g = m.segments[static_cast<std::size_t>(t.first_segment + r)];
+        if (g.bit_width > max_bits || (m.image.type == PixelType::uint16 && g.seed > UINT16_MAX) ||
+            g.payload_offset < format::segment_header_bytes || g.payload_offset % 4 != 0 ||
+            g.payload_offset > t.length || g.payload_bytes > t.length - g.payload_offset ||
+            g.payload_bytes != ((w - 1) * g.bit_width + 31) / 32 * 4) {
+            return Status::malformed_data;
+        }
+    }
+    return Status::success;
+}
+
+// The ROI clip of one tile: rows [row0, row1) and columns [col0, col1) of the tile, placed at
+// output (ox, oy).
+void clip(tsk_decode_task &t, const Roi &roi, std::uint64_t x, std::uint64_t y) {
+    const std::uint64_t rx1 = std::uint64_t{roi.x} + roi.width;
+    const std::uint64_t ry1 = std::uint64_t{roi.y} + roi.height;
+    t.row0 = static_cast<std::uint16_t>(roi.y > y ? roi.y - y : 0);
+    t.row1 = static_cast<std::uint16_t>(ry1 < y + t.height ? ry1 - y : t.height);
+    t.col0 = static_cast<std::uint16_t>(roi.x > x ? roi.x - x : 0);
+    t.col1 = static_cast<std::uint16_t>(rx1 < x + t.width ? rx1 - x : t.width);
+    t.ox = static_cast<std::uint32_t>(x + t.col0 - roi.x);
+    t.oy = static_cast<std::uint32_t>(y + t.row0 - roi.y);
+}
+
+// Selects the tiles that intersect the region (row-major) and rebases them into the supplied
+// bytes (reference plan.cpp:281-349).
+Status stage_tiles(const CompressedInput &src, const Roi &roi, std::uint32_t image,
+                   std::uint8_t flags, Draft &d) {
+    const ImageMetadata &m = *src.metadata;
+    const std::uint64_t across = tiles_across(m.image, m.tile);
+    if (m.tiles.size() != across * tiles_down(m.image, m.tile)) {
+        return Status::malformed_data;
+    }
+    const std::uint64_t left = roi.x / m.tile.width;
+    const std::uint64_t right = (std::uint64_t{roi.x} + roi.width - 1) / m.tile.width;
+    const std::uint64_t top = roi.y / m.tile.height;
+    const std::uint64_t bottom = (std::uint64_t{roi.y} + roi.height - 1) / m.tile.height;
+    const std::uint64_t selected = (right - left + 1) * (bottom - top + 1);
+    const bool mapped = src.mappings != nullptr || src.mapping_count != 0;
+    if (mapped ? src.mappings == nullptr || src.mapping_count != selected
+               : m.file_bytes > src.bytes.size) {
+        return mapped ? Status::invalid_argument : Status::buffer_too_small;
+    }
+    std::vector<Range> staged;
+    const auto *base = static_cast<const std::uint8_t *>(src.bytes.data);
+    std::uint64_t k = 0;
+    for (std::uint64_t row = top; row <= bottom; ++row) {
+        for (std::uint64_t col = left; col <= right; ++col, ++k) {
+            const std::uint64_t index = row * across + col;
+            const Status st = check_tile(m, index);
+            if (st != Status::success) {
+                return st;
+            }
+            const TileMetadata &t = m.tiles[static_cast<std::size_t>(index)];
+            std::uint64_t offset = t.offset;
+            if (mapped) {
+                const TileMapping &map = src.mappings[k];
+                if (map.tile_index != index || map.input_offset % 4 != 0 ||
+                    map.input_offset > src.bytes.size ||
+                    t.length > src.bytes.size - map.input_offset) {
+                    return Status::invalid_argument;
+                }
+                offset = map.input_offset;
+                staged.push_back({static_cast<std::uintptr_t>(offset),
+                                  static_cast<std::uintptr_t>(offset + t.length)});
+            }
+            tsk_decode_task task{};
+            task.src = reinterpret_cast<std::uint64_t>(base + offset);
+            task.words_or_tile = t.length / 4;
+            task.image = image;
+            task.width = t.width;
+            task.height = t.height;
+            task.mode = static_cast<std::uint8_t>(t.mode);
+            task.flags = flags | (k == 0 ? TSK_FIRST : 0);
+            clip(task, roi, col * m.tile.width, row * m.tile.height);
+            if (t.mode == TileMode::predict_bitpack) {
+                task.rows_at = static_cast<std::uint32_t>(d.rows.size());
+                d.rows.resize(d.rows.size() + TSK_ROW_SLOT, 0);
+                for (std::uint64_t r = 0; r < t.height; ++r) {
+                    const SegmentMetadata &g =
+                        m.segments[static_cast<std::size_t>(t.first_segment + r)];
+                    // Word index of the row descriptor within the tile payload.
+                    d.rows[task.rows_at + r] = static_cast<tsk_row_start>(
+                        (g.payload_offset - format::segment_header_bytes) / 4);
+                }
+            }
+            d.tasks.push_back(task);
+        }
+    }
+    std::sort(staged.begin(), staged.end(),
+              [](const Range &a, const Range &b) { return a.begin < b.begin; });
+    for (std::size_t i = 1; i < staged.size(); ++i) {
+        if (staged[i].begin < staged[i - 1].end) {
+            return Status::invalid_argument;
+        }
+    }
+    d.tiles_per_image.push_back(selected);
+    return Status::success;
+}
+
+Status draft_decode(const BatchRequest &request, Draft &d) {
+    bool mixed = false;
+    const bool calibrated = request.operation == Operation::decode_calibrate;
+    for (std::uint64_t i = 0; i < request.count; ++i) {
+        const BatchItem &item = request.items[i];
+        const CompressedInput &src = item.compressed_input;
+        const bool trusted = src.encoder_result != nullptr;
+        if (trusted ? src.metadata != nullptr || src.mappings != nullptr || src.mapping_count != 0
+                    : src.metadata == nullptr) {
+            return Status::invalid_argument;
+        }
+        const ImageSpec image = trusted ? src.trusted_image : src.metadata->image;
+        const TileShape shape = trusted ? src.trusted_tile : src.metadata->tile;
+        std::uint64_t bound = 0;
+        Status st = compress_bound(image, shape, bound);
+        if (st != Status::success) {
+            return st;
+        }
+        if (i == 0) {
+            d.type = image.type;
+            d.shape = shape;
+        }
+        if (image.type != d.type) {
+            return Status::invalid_argument;
+        }
+        mixed = mixed || shape.width != d.shape.width || shape.height != d.shape.height;
+        const ImageView &out = item.output;
+        st = host::view_ok(out);
+        if (st != Status::success) {
+            return st;
+        }
+        Roi roi{0, 0, image.width, image.height};
+        if (request.operation != Operation::decompress) {
+            roi = item.roi;
+            if (roi.width == 0 || roi.height == 0 ||
+                std::uint64_t{roi.x} + roi.width > image.width ||
+                std::uint64_t{roi.y} + roi.height > image.height) {
+                return Status::invalid_roi;
+            }
+        }
+        if (out.image.type != (calibrated ? PixelType::float32 : image.type) ||
+            out.image.width != roi.width || out.image.height != roi.height) {
+            return Status::invalid_argument;
+        }
+        if (calibrated) {
+            st = check_calibration(item.calibration, out.image, d);
+            if (st != Status::success) {
+                return st;
+            }
+        }
+        st = host::byte_range(src.bytes.data, src.bytes.size);
+        if (st != Status::success) {
+            return st;
+        }
+        if (src.bytes.data == nullptr || reinterpret_cast<std::uintptr_t>(src.bytes.data) % 4 != 0) {
+            return Status::invalid_argument;
+        }
+
+        const auto index = static_cast<std::uint32_t>(d.images.size());
+        tsk_decode_image rec{};
+        rec.out = reinterpret_cast<std::uint64_t>(out.data);
+        rec.out_pitch = out.pitch_bytes;
+        rec.gain = 1.0f;
+        if (calibrated) {
+            set_parameters(item.calibration, rec.offset_map, rec.offset_pitch, rec.offset,
+                           rec.gain_map, rec.gain_pitch, rec.gain);
+        }
+        const std::uint64_t out_sample = calibrated ? 4 : (image.type == PixelType::uint16 ? 2 : 4);
+        rec.result_bytes = std::uint64_t{roi.width} * roi.height * out_sample;
+        rec.archive_width = image.width;
+        rec.archive_height = image.height;
+        rec.tile_width = shape.width;
+        rec.tile_height = shape.height;
+        std::uint8_t flags = (image.type == PixelType::float32 ? TSK_F32 : 0) |
+                             (calibrated ? TSK_CALIBRATED : 0);
+        const std::size_t first_task = d.tasks.size();
+        if (trusted) {
+            if (reinterpret_cast<std::uintptr_t>(src.encoder_result) % alignof(DeviceResult) != 0) {
+                return Status::invalid_argument;
+            }
+            if (src.bytes.size < bound) {
+                return Status::buffer_too_small;
+            }
+            const std::uint64_t across = tiles_across(image, shape);
+            const std::uint64_t top = roi.y / shape.height;
+            const std::uint64_t bottom = (std::uint64_t{roi.y} + roi.height - 1) / shape.height;
+            const std::uint64_t left = roi.x / shape.width;
+            const std::uint64_t right = (std::uint64_t{roi.x} + roi.width - 1) / shape.width;
+            for (std::uint64_t row = top; row <= bottom; ++row) {
+                for (std::uint64_t col = left; col <= right; ++col) {
+                    tsk_decode_task task{};
+                    const std::uint64_t x = col * shape.width, y = row * shape.height;
+                    task.src = reinterpret_cast<std::uint64_t>(src.bytes.data);
+                    task.words_or_tile = row * across + col;
+                    task.image = index;
+                    task.width = static_cast<std::uint16_t>(
+                        std::min<std::uint64_t>(shape.width, image.width - x));
+                    task.height = static_cast<std::uint16_t>(
+                        std::min<std::uint64_t>(shape.height, image.height - y));
+                    task.flags = flags | TSK_TRUSTED;
+                    clip(task, roi, x, y);
+                    d.tasks.push_back(task);
+                }
+            }
+            d.tiles_per_image.push_back(d.tasks.size() - first_task);
+            rec.encoder_result = reinterpret_cast<std::uint64_t>(src.encoder_result);
+            rec.capacity = src.bytes.size;
+            d.trusted = true;
+            d.readable.push_back(range_of(src.encoder_result, sizeof(DeviceResult)));
+            d.pointers.push_back(src.encoder_result);
+        } else {
+            st = stage_tiles(src, roi, index, flags, d);
+            if (st != Status::success) {
+                return st;
+            }
+        }
+        const std::uint64_t ntasks = d.tasks.size() - first_task;
+        if (ntasks > UINT32_MAX) {
+            return Status::resource_limit;
+        }
+        rec.tile_count = static_cast<std::uint32_t>(ntasks);
+        d.images.push_back(rec);
+        d.readable.push_back(range_of(src.bytes.data, src.bytes.size));
+        d.writable.push_back(range_of(out.data, out.capacity_bytes));
+        d.pointers.push_back(src.bytes.data);
+        d.pointers.push_back(out.data);
+    }
+    if (mixed) {
+        d.shape = {64, 64}; // the geometry with the most rows bounds every window
+    }
+    return Status::success;
+}
+
+// The reference's window accounting (plan.cpp:467-491, 542-555): maxima of images and tiles over
+// sequential windows of at most 4096 tiles.
+void window_spec(const std::vector<std::uint64_t> &tiles, WorkspaceSpec &spec) {
+    std::uint64_t used = 0, images = 0, count = 0;
+    bool open = false;
+    auto close = [&]() {
+        if (open) {
+            spec.image_count = std::max(spec.image_count, images);
+            spec.tile_count = std::max(spec.tile_count, count);
+        }
+    };
+    for (std::uint64_t n : tiles) {
+        for (std::uint64_t start = 0; start < n;) {
+            if (!open || used == kWindowTiles) {
+                close();
+                open = true;
+                used = images = count = 0;
+            }
+            const std::uint64_t take = std::min<std::uint64_t>(n - start, kWindowTiles - used);
+            ++images;
+            count += take;
+            used += take;
+            start += take;
+        }
+    }
+    close();
+}
+
+template <typename T>
+bool place(std::uint64_t &total, const std::vector<T> &v, std::uint64_t &at) {
+    std::uint64_t bytes = 0;
+    return host::align_up(total, 256, at) && host::mul(v.size(), sizeof(T), bytes) &&
+           host::add(at, bytes, total);
+}
+
+template <typename T>
+bool upload(void *storage, std::uint64_t at, const std::vector<T> &v, cudaStream_t stream) {
+    return v.empty() || cudaMemcpyAsync(static_cast<std::uint8_t *>(storage) + at, v.data(),
+                                        v.size() * sizeof(T), cudaMemcpyHostToDevice,
+                                        stream) == cudaSuccess;
+}
+
+Status build(const BatchRequest &request, PlanState &plan, cudaStream_t stream) {
+    plan.operation = request.operation;
+    plan.count = request.count;
+    if (request.count == 0) {
+        return Status::success;
+    }
+    Draft d;
+    Status st = request.operation == Operation::compress    ? draft_compress(request, d)
+                : request.operation == Operation::calibrate ? draft_calibrate(request, d)
+                                                            : draft_decode(request, d);
+    if (st != Status::success) {
+        return st;
+    }
+    plan.type = d.type;
+    if (!plan.ranges.assign(std::move(d.writable), std::move(d.readable))) {
+        return Status::invalid_argument;
+    }
+    int pageable = 0;
+    if (cudaGetDevice(&plan.device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&pageable, cudaDevAttrPageableMemoryAccess, plan.device) !=
+            cudaSuccess) {
+        return cuda_failure();
+    }
+    plan.pageable = pageable != 0;
+    st = stream_device(stream, plan.device);
+    if (st != Status::success) {
+        return st;
+    }
+    for (const void *p : d.pointers) {
+        st = accessible(p, plan.device, plan.pageable);
+        if (st != Status::success) {
+            return st;
+        }
+    }
+
+    plan.spec = {0, 0, d.shape, 0};
+    if (request.operation != Operation::calibrate) {
+        window_spec(d.tiles_per_image, plan.spec);
+    }
+    if (request.operation == Operation::compress) {
+        // This encoder's own device-wide primitive: the look-back flags of every tile.
+        plan.spec.scan_temp_bytes = tsk_encode_state_bytes(d.total_tiles);
+    }
+    st = host::workspace_layout(plan.spec, plan.layout);
+    if (st != Status::success) {
+        return st;
+    }
+    if (d.tasks.size() > UINT32_MAX || d.calib_tasks.size() > UINT32_MAX) {
+        return Status::resource_limit;
+    }
+
+    std::uint64_t total = 0, at_images = 0, at_tasks = 0, at_rows = 0, at_enc = 0, at_cal_images = 0,
+                  at_cal_tasks = 0;
+    if (!place(total, d.images, at_images) || !place(total, d.tasks, at_tasks) ||
+        !place(total, d.rows, at_rows) || !place(total, d.encode_images, at_enc) ||
+        !place(total, d.calib_images, at_cal_images) ||
+        !place(total, d.calib_tasks, at_cal_tasks)) {
+        return Status::size_overflow;
+    }
+    if (cudaMallocAsync(&plan.storage, static_cast<std::size_t>(total), stream) != cudaSuccess) {
+        plan.storage = nullptr;
+        return cuda_failure();
+    }
+    auto *dev = static_cast<std::uint8_t *>(plan.storage);
+    plan.images = reinterpret_cast<const tsk_decode_image *>(dev + at_images);
+    plan.tasks = reinterpret_cast<const tsk_decode_task *>(dev + at_tasks);
+    plan.task_count = static_cast<std::uint32_t>(d.tasks.size());
+    plan.rows = reinterpret_cast<const tsk_row_start *>(dev + at_rows);
+    plan.trusted = d.trusted;
+    plan.encode_images = reinterpret_cast<const tsk_encode_image *>(dev + at_enc);
+    plan.total_tiles = d.total_tiles;
+    plan.calib_images = reinterpret_cast<const tsk_calib_image *>(dev + at_cal_images);
+    plan.calib_tasks = reinterpret_cast<const tsk_calib_task *>(dev + at_cal_tasks);
+    plan.calib_task_count = static_cast<std::uint32_t>(d.calib_tasks.size());
+
+    // Load every kernel the plan launches now, so no execution has to (docs/api.md:69).
+    int err = 0;
+    switch (request.operation) {
+    case Operation::compress:
+        err = tsk_encode_prepare(plan.device);
+        break;
+    case Operation::calibrate:
+        err = tsk_calibrate_prepare(plan.device);
+        break;
+    default:
+        plan.config.group = 4;
+        err = tsk_decode_prepare(&plan.config, plan.task_count, plan.device);
+        break;
+    }
+    if (err != 0) {
+        return cuda_failure();
+    }
+    if (!upload(plan.storage, at_images, d.images, stream) ||
+        !upload(plan.storage, at_tasks, d.tasks, stream) ||
+        !upload(plan.storage, at_rows, d.rows, stream) ||
+        !upload(plan.storage, at_enc, d.encode_images, stream) ||
+        !upload(plan.storage, at_cal_images, d.calib_images, stream) ||
+        !upload(plan.storage, at_cal_tasks, d.calib_tasks, stream) ||
+        cudaStreamSynchronize(stream) != cudaSuccess) {
+        return cuda_failure();
+    }
+    return Status::success;
+}
+
+} // namespace
+
+Status check_execution(const PlanState *plan, Operation operation, MutableBytes workspace,
+                       ResultBuffer results, cudaStream_t stream) noexcept {
+    if (plan == nullptr || plan->operation != operation) {
+        return Status::invalid_argument;
+    }
+    if (plan->count == 0) {
+        return Status::success;
+    }
+    std::uint64_t result_bytes = 0;
+    if (!host::mul(results.count, sizeof(DeviceResult), result_bytes)) {
+        return Status::size_overflow;
+    }
+    Status st = host::byte_range(workspace.data, workspace.size);
+    if (st == Status::success) {
+        st = host::byte_range(results.data, result_bytes);
+    }
+    if (st != Status::success) {
+        return st;
+    }
+    if (workspace.size < plan->layout.total || results.count < plan->count) {
+        return Status::buffer_too_small;
+    }
+    if (reinterpret_cast<std::uintptr_t>(workspace.data) % workspace_alignment != 0 ||
+        reinterpret_cast<std::uintptr_t>(results.data) % alignof(DeviceResult) != 0) {
+        return Status::invalid_argument;
+    }
+    const Range scratch = range_of(workspace.data, workspace.size);
+    const Range records = range_of(results.data, result_bytes);
+    if (!plan->ranges.disjoint(scratch) || !plan->ranges.disjoint(records) ||
+        host::overlaps(workspace.data, workspace.size, results.data, result_bytes)) {
+        return Status::invalid_argument;
+    }
+    st = stream_device(stream, plan->device);
+    if (st == Status::success && workspace.size != 0) {
+        st = accessible(workspace.data, plan->device, plan->pageable);
+    }
+    if (st == Status::success) {
+        st = accessible(results.data, plan->device, plan->pageable);
+    }
+    // A pending error from the caller's own work is left for the caller (docs/api.md:160).
+    if (st == Status::success && cudaPeekAtLastError() != cudaSuccess) {
+        st = Status::cuda_error;
+    }
+    return st;
+}
+
+} // namespace detail
+
+BatchPlan::BatchPlan(std::unique_ptr<Impl> impl) noexcept : impl_(std::move(impl)) {}
+BatchPlan::~BatchPlan() = default;
+BatchPlan::BatchPlan(BatchPlan &&) noexcept = default;
+BatchPlan &BatchPlan::operator=(BatchPlan &&) noexcept = default;
+
+WorkspaceSpec BatchPlan::workspace_spec() const noexcept {
+    return impl_ != nullptr ? impl_->spec : WorkspaceSpec{};
+}
+
+Status prepare_batch(const BatchRequest &request, std::unique_ptr<BatchPlan> &plan,
+                     cudaStream_t stream) noexcept {
+    if (request.count > UINT32_MAX) {
+        return Status::resource_limit;
+    }
+    if (request.count != 0 && request.items == nullptr) {
+        return Status::invalid_argument;
+    }
+    if (request.operation > Operation::decode_calibrate) {
+        return Status::invalid_argument;
+    }
+    try {
+        auto impl = std::make_unique<BatchPlan::Impl>();
+        const Status st = detail::build(request, *impl, stream);
+        if (st != Status::success) {
+            return st;
+        }
+        plan.reset(new BatchPlan(std::move(impl)));
+        return Status::success;
+    } catch (const std::bad_alloc &) {
+        return Status::resource_limit;
+    } catch (const std::length_error &) {
+        return Status::resource_limit;
+    }
+}
+
+namespace {
+
+Status run_decode(const BatchPlan &plan, Operation op, MutableBytes workspace,
+                  ResultBuffer results, cudaStream_t stream) noexcept {
+    const detail::PlanState *p = PlanAccess::state(plan);
+    const Status st = detail::check_execution(p, op, workspace, results, stream);
+    if (st != Status::success || p->count == 0) {
+        return st;
+    }
+    auto *records = reinterpret_cast<tsk_result *>(results.data);
+    if (p->trusted &&
+        cudaMemsetAsync(records, 0, sizeof(tsk_result) * p->count, stream) != cudaSuccess) {
+        return detail::cuda_failure();
+    }
+    return detail::cuda_status(
+        tsk_decode_launch(p->tasks, p->task_count, p->images, p->rows, records, p->config, stream));
+}
+
+} // namespace
+
+Status decompress_async(const BatchPlan &plan, MutableBytes workspace, ResultBuffer results,
+                        cudaStream_t stream) noexcept {
+    return run_decode(plan, Operation::decompress, workspace, results, stream);
+}
+
+Status decode_roi_async(const BatchPlan &plan, MutableBytes workspace, ResultBuffer results,
+                        cudaStream_t stream) noexcept {
+    return run_decode(plan, Operation::decode_roi, workspace, results, stream);
+}
+
+Status decode_calibrate_async(const BatchPlan &plan, MutableBytes workspace, ResultBuffer results,
+                              cudaStream_t stream) noexcept {
+    return run_decode(plan, Operation::decode_calibrate, workspace, results, stream);
+}
+
+Status compress_async(const BatchPlan &plan, MutableBytes workspace, ResultBuffer results,
+                      cudaStream_t stream) noexcept {
+    const detail::PlanState *p = PlanAccess::state(plan);
+    const Status st = detail::check_execution(p, Operation::compress, workspace, results, stream);
+    if (st != Status::success || p->count == 0) {
+        return st;
+    }
+    void *state = static_cast<std::uint8_t *>(workspace.data) + p->layout.temp;
+    return detail::cuda_status(tsk_encode_launch(
+        p->encode_images, static_cast<std::uint32_t>(p->count), p->total_tiles, 0, state,
+        reinterpret_cast<tsk_result *>(results.data), stream));
+}
+
+Status calibrate_async(const BatchPlan &plan, MutableBytes workspace, ResultBuffer results,
+                       cudaStream_t stream) noexcept {
+    const detail::PlanState *p = PlanAccess::state(plan);
+    const Status st = detail::check_execution(p, Operation::calibrate, workspace, results, stream);
+    if (st != Status::success || p->count == 0) {
+        return st;
+    }
+    return detail::cuda_status(tsk_calibrate_launch(
+        p->calib_tasks, p->calib_task_count, p->calib_images, static_cast<std::uint32_t>(p->count),
+        reinterpret_cast<tsk_result *>(results.data), stream));
+}
+
+} // namespace tilestream::cuda

@@ -1,0 +1,106 @@
+// Internal plan state behind tilestream::cuda::BatchPlan.
+#pragma once
+
+#include <tilestream/cuda.h>
+
+#include "../kernels/tasks.h"
+#include "checked.h"
+
+#include <cstdint>
+#include <vector>
+
+namespace tilestream::cuda::detail {
+
+struct Range {
+    std::uintptr_t begin = 0;
+    std::uintptr_t end = 0;
+};
+
+// Writable ranges are pairwise disjoint and disjoint from every readable range; readable
+// ranges may overlap one another (docs/api.md:146-148).
+class RangeSet {
+  public:
+    [[nodiscard]] bool assign(std::vector<Range> writable, std::vector<Range> readable);
+    [[nodiscard]] bool disjoint(Range range) const noexcept;
+
+  private:
+    std::vector<Range> writable_;
+    std::vector<Range> readable_;
+    std::vector<std::uintptr_t> max_end_; // max end of readable_[0..i]
+};
+
+inline Range range_of(const void *data, std::uint64_t size) noexcept {
+    const auto b = reinterpret_cast<std::uintptr_t>(data);
+    return {b, b + static_cast<std::uintptr_t>(size)};
+}
+
+// A CUDA failure is reported through Status; the error is cleared so a later check cannot
+// blame it on another launch (reference plan.h:84-91).
+inline Status cuda_failure() noexcept {
+    static_cast<void>(cudaGetLastError());
+    return Status::cuda_error;
+}
+
+inline Status cuda_status(cudaError_t e) noexcept {
+    return e == cudaSuccess ? Status::success : cuda_failure();
+}
+
+inline Status cuda_status(int e) noexcept {
+    return cuda_status(static_cast<cudaError_t>(e));
+}
+
+[[nodiscard]] Status accessible(const void *data, int device, bool pageable) noexcept;
+[[nodiscard]] Status stream_device(cudaStream_t stream, int device) noexcept;
+
+struct PlanState {
+    Operation operation = Operation::compress;
+    PixelType type = PixelType::uint16;
+    int device = 0;
+    bool pageable = false;
+    std::uint64_t count = 0;
+    WorkspaceSpec spec;
+    host::WorkspaceLayout layout;
+    RangeSet ranges;
+    void *storage = nullptr; // one device allocation holding every table
+
+    // Decode.
+    const tsk_decode_task *tasks = nullptr;
+    std::uint32_t task_count = 0;
+    const tsk_decode_image *images = nullptr;
+    const tsk_row_start *rows = nullptr;
+    tsk_decode_config config{};
+    bool trusted = false;
+
+    // Encode.
+    const tsk_encode_image *encode_images = nullptr;
+    std::uint64_t total_tiles = 0;
+
+    // Standalone calibration.
+    const tsk_calib_task *calib_tasks = nullptr;
+    std::uint32_t calib_task_count = 0;
+    const tsk_calib_image *calib_images = nullptr;
+
+    PlanState() = default;
+    PlanState(const PlanState &) = delete;
+    PlanState &operator=(const PlanState &) = delete;
+    ~PlanState();
+};
+
+[[nodiscard]] Status check_execution(const PlanState *plan, Operation operation,
+                                     MutableBytes workspace, ResultBuffer results,
+                                     cudaStream_t stream) noexcept;
+
+} // namespace tilestream::cuda::detail
+
+namespace tilestream::cuda {
+
+struct BatchPlan::Impl final : detail::PlanState {};
+
+// Access to plan internals for the library's own extensions (C entry layer, batching).
+struct PlanAccess {
+    static const detail::PlanState *state(const BatchPlan &plan) noexcept {
+        return plan.impl_.get();
+    }
+};
+
+} // namespace tilestream::cuda

@@ -1,0 +1,156 @@
+// Execution records shared by the host planner and the sm_100a kernels, and the internal
+// extern "C" launcher layer between them. Plain C layout: no C++ types cross this boundary.
+//
+// The planner flattens every batch into one queue of self-contained tile tasks, so a kernel
+// never searches for the image that owns a block (the reference binary-searches window entries
+// per block, src/cuda/device.cuh:32-45).
+#pragma once
+
+#include <cuda_runtime_api.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    TSK_RAW = 0,
+    TSK_CONSTANT = 1,
+    TSK_PREDICT = 2,
+};
+
+// DecodeTask.flags
+enum {
+    TSK_F32 = 1,        // samples are FP32 words (else uint16)
+    TSK_CALIBRATED = 2, // output is calibrated FP32
+    TSK_TRUSTED = 4,    // index entry and rows are read on the device (encoder output)
+    TSK_FIRST = 8,      // first task of its image: writes the image's result record
+};
+
+// Largest payload of one tile: RAW FP32, 4096 samples.
+#define TSK_TILE_PIXELS 4096
+#define TSK_MAX_ROWS 64
+#define TSK_PAYLOAD_BYTES 16384
+
+// One tile to decode. 48 bytes.
+typedef struct __align__(16) {
+    // Parsed: device address of the tile payload. Trusted: device address of the archive.
+    uint64_t src;
+    // Parsed: payload length in 32-bit words. Trusted: the tile's index in the archive.
+    uint64_t words_or_tile;
+    uint32_t image;   // slot in the image table and the result buffer
+    uint32_t rows_at; // parsed PREDICT: first entry of this tile's row table
+    uint32_t ox;      // output column of tile column col0
+    uint32_t oy;      // output row of tile row row0
+    uint16_t width;   // actual tile width
+    uint16_t height;  // actual tile height
+    uint16_t row0, row1; // tile rows written: [row0, row1)
+    uint16_t col0, col1; // tile columns written: [col0, col1)
+    uint8_t mode;        // parsed: TSK_RAW/CONSTANT/PREDICT
+    uint8_t flags;
+    uint16_t reserved;
+} tsk_decode_task;
+
+// Per-image state of a decode execution. 96 bytes.
+typedef struct __align__(16) {
+    uint64_t out;   // output base (device address)
+    uint64_t out_pitch;
+    uint64_t offset_map; // 0 when the offset is a scalar
+    uint64_t offset_pitch;
+    uint64_t gain_map; // 0 when the gain is a scalar
+    uint64_t gain_pitch;
+    uint64_t result_bytes;   // bytes_written reported on success
+    uint64_t encoder_result; // trusted: producing DeviceResult (device address), else 0
+    uint64_t capacity;       // trusted: capacity of the archive buffer in bytes
+    float offset;
+    float gain;
+    uint32_t tile_count; // tasks of this image (trusted completion count)
+    uint32_t archive_width;  // trusted: archive geometry
+    uint32_t archive_height;
+    uint16_t tile_width, tile_height;
+} tsk_decode_image;
+
+// Row table entry (parsed PREDICT tiles): word index of the row descriptor within the tile
+// payload. Each tile's rows occupy one 16-byte-aligned slot of TSK_MAX_ROWS entries so that the
+// slot can be staged with one bulk copy.
+typedef uint16_t tsk_row_start;
+#define TSK_ROW_SLOT TSK_MAX_ROWS
+
+// Launch parameters chosen by the planner (and by the autotuner for batches).
+typedef struct {
+    uint32_t grid;   // persistent CTAs
+    uint32_t group;  // columns per lane: 4 or 8
+    uint32_t stages; // staging depth: 2 or 3 (fixed by the kernel build)
+    uint32_t reserved;
+} tsk_decode_config;
+
+// One image to encode. 96 bytes.
+typedef struct __align__(16) {
+    uint64_t input;  // device address of pixel (0, 0)
+    uint64_t pitch;
+    uint64_t output; // device address of the .tsc file buffer
+    uint64_t tile_count;
+    uint64_t first_tile; // index of this image's first tile in the batch's tile sequence
+    uint32_t width, height;
+    uint16_t tile_width, tile_height;
+    uint32_t type; // 1 = uint16, 2 = float32
+    uint64_t columns;
+    uint64_t reserved[3];
+} tsk_encode_image;
+
+// One standalone-calibration chunk: rows [y0, y0 + rows) of one image. 16 bytes.
+typedef struct __align__(16) {
+    uint32_t image;
+    uint32_t y0;
+    uint32_t rows;
+    uint32_t reserved;
+} tsk_calib_task;
+
+// Per-image calibration state. 96 bytes.
+typedef struct __align__(16) {
+    uint64_t input;
+    uint64_t in_pitch;
+    uint64_t out;
+    uint64_t out_pitch;
+    uint64_t offset_map;
+    uint64_t offset_pitch;
+    uint64_t gain_map;
+    uint64_t gain_pitch;
+    float offset, gain;
+    uint32_t width, height;
+    uint32_t type;
+    uint32_t reserved[3];
+} tsk_calib_image;
+
+// DeviceResult as seen by the kernels (types.h: {status, reserved, bytes_written}).
+typedef struct {
+    uint32_t status;
+    uint32_t reserved;
+    uint64_t bytes_written;
+} tsk_result;
+
+// --- launchers: return a cudaError_t value (0 = enqueued) ----------------------------------
+
+// Decodes ntasks tasks. results: one record per image. zero_results: the planner has enqueued
+// a clear of the result records (needed by trusted images, whose completion is counted).
+int tsk_decode_launch(const tsk_decode_task *tasks, uint32_t ntasks,
+                      const tsk_decode_image *images, const tsk_row_start *rows,
+                      tsk_result *results, tsk_decode_config config, cudaStream_t stream);
+// Occupancy-derived persistent grid for a decode launch, and the kernel preload.
+int tsk_decode_prepare(tsk_decode_config *config, uint32_t ntasks, int device);
+
+// Encodes every tile of every image in one pass. state: 8 * (total_tiles + 2) bytes of
+// workspace, cleared by the launcher in stream order.
+int tsk_encode_launch(const tsk_encode_image *images, uint32_t image_count, uint64_t total_tiles,
+                      uint32_t any_float, void *state, tsk_result *results, cudaStream_t stream);
+int tsk_encode_prepare(int device);
+uint64_t tsk_encode_state_bytes(uint64_t total_tiles);
+
+int tsk_calibrate_launch(const tsk_calib_task *tasks, uint32_t ntasks,
+                         const tsk_calib_image *images, uint32_t image_count, tsk_result *results,
+                         cudaStream_t stream);
+int tsk_calibrate_prepare(int device);
+
+#ifdef __cplusplus
+}
+#endif

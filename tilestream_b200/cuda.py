@@ -1,0 +1,122 @@
+"""Python mirror of include/tilestream/cuda.h: plan preparation and the five executors.
+
+Device buffers are any objects with a device address (torch CUDA tensors, or addresses from
+`allocate`); streams are CUDA stream handles (int) or torch.cuda.Stream objects.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import enum
+
+from . import _native as N
+from .api import (BatchItem, BatchRequest, MutableBytes, ResultBuffer, Status, TileShape,
+                  WorkspaceSpec, workspace_size)
+
+
+class Operation(enum.IntEnum):
+    compress = 0
+    decompress = 1
+    decode_roi = 2
+    calibrate = 3
+    decode_calibrate = 4
+
+
+class ParameterKind(enum.IntEnum):
+    scalar = 0
+    map = 1
+
+
+def stream_handle(stream) -> int:
+    if stream is None:
+        return 0
+    if hasattr(stream, "cuda_stream"):
+        return int(stream.cuda_stream)
+    return int(stream)
+
+
+class BatchPlan:
+    """An owned tilestream::cuda::BatchPlan."""
+
+    def __init__(self, handle: int):
+        self.handle = handle
+
+    def workspace_spec(self) -> WorkspaceSpec:
+        spec = WorkspaceSpec()
+        N.lib().ts_plan_workspace_spec(self.handle, C.byref(spec))
+        return spec
+
+    def workspace_bytes(self) -> int:
+        st, n = workspace_size(self.workspace_spec())
+        if st != Status.success:
+            raise RuntimeError(f"workspace_size: {st!r}")
+        return n
+
+    def __del__(self):
+        if getattr(self, "handle", None):
+            N.lib().ts_plan_destroy(self.handle)
+            self.handle = None
+
+
+def make_request(operation, items, tile: TileShape | None = None) -> BatchRequest:
+    items = list(items)
+    arr = (BatchItem * max(1, len(items)))(*items)
+    req = BatchRequest(int(operation), C.cast(arr, C.POINTER(BatchItem)) if items else None,
+                       len(items), tile if tile is not None else TileShape())
+    req._keep = arr  # the item array must outlive prepare_batch
+    return req
+
+
+def prepare_batch(request: BatchRequest, plan: BatchPlan | None = None, stream=None):
+    """Returns (Status, plan). On failure the previous plan (if any) is returned unchanged."""
+    h = C.c_void_p(0)
+    st = N.lib().ts_prepare_batch(C.byref(request), C.byref(h), stream_handle(stream))
+    if st == 0:
+        return Status.success, BatchPlan(h.value)
+    return Status(st), plan
+
+
+def _results(results) -> ResultBuffer:
+    if isinstance(results, ResultBuffer):
+        return results
+    from .api import _ptr, nbytes
+    return ResultBuffer(_ptr(results), nbytes(results) // 16)
+
+
+def _workspace(workspace) -> MutableBytes:
+    if isinstance(workspace, MutableBytes):
+        return workspace
+    if workspace is None:
+        return MutableBytes(None, 0)
+    from .api import mutable_bytes
+    return mutable_bytes(workspace)
+
+
+def _executor(name):
+    def run(plan: BatchPlan, workspace, results, stream=None) -> Status:
+        fn = getattr(N.lib(), name)
+        return Status(fn(plan.handle if plan is not None else None, _workspace(workspace),
+                         _results(results), stream_handle(stream)))
+    run.__name__ = name[3:]
+    return run
+
+
+compress_async = _executor("ts_compress_async")
+decompress_async = _executor("ts_decompress_async")
+decode_roi_async = _executor("ts_decode_roi_async")
+calibrate_async = _executor("ts_calibrate_async")
+decode_calibrate_async = _executor("ts_decode_calibrate_async")
+
+
+def synchronize(stream=None) -> Status:
+    return Status(N.lib().ts_synchronize(stream_handle(stream)))
+
+
+def allocate(nbytes: int, stream=None):
+    """DeviceBuffer::allocate: returns (Status, device address)."""
+    p = C.c_void_p(0)
+    st = N.lib().ts_device_allocate(nbytes, stream_handle(stream), C.byref(p))
+    return Status(st), (p.value or 0)
+
+
+def release(address: int, stream=None) -> Status:
+    return Status(N.lib().ts_device_release(address, stream_handle(stream)))
