@@ -11,6 +11,8 @@
 #include "plan.h"
 
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <stdexcept>
@@ -74,10 +76,19 @@ PlanState::~PlanState() {
     }
 }
 
+void log_failure(const char *what, cudaError_t error) noexcept {
+    static const bool enabled = std::getenv("TILESTREAM_DEBUG") != nullptr;
+    if (enabled) {
+        std::fprintf(stderr, "tilestream: %s failed: %s (%d)\n", what, cudaGetErrorName(error),
+                     static_cast<int>(error));
+    }
+}
+
 Status accessible(const void *data, int device, bool pageable) noexcept {
     cudaPointerAttributes a{};
-    if (cudaPointerGetAttributes(&a, data) != cudaSuccess) {
-        return cuda_failure();
+    const cudaError_t e = cudaPointerGetAttributes(&a, data);
+    if (e != cudaSuccess) {
+        return cuda_failure("cudaPointerGetAttributes", e);
     }
     switch (a.type) {
     case cudaMemoryTypeDevice:
@@ -93,8 +104,25 @@ Status accessible(const void *data, int device, bool pageable) noexcept {
 
 Status stream_device(cudaStream_t stream, int device) noexcept {
     int current = 0, owner = 0;
-    if (cudaGetDevice(&current) != cudaSuccess || cudaStreamGetDevice(stream, &owner) != cudaSuccess) {
-        return cuda_failure();
+    cudaError_t e = cudaGetDevice(&current);
+    if (e != cudaSuccess) {
+        return cuda_failure("cudaGetDevice", e);
+    }
+    // A stream that is being captured into a CUDA graph cannot be asked for its device
+    // (cudaErrorStreamCaptureUnsupported); the capture then checks the current device only and
+    // the launch itself rejects a stream of another device.
+    cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+    e = cudaStreamIsCapturing(stream, &capture);
+    if (e != cudaSuccess) {
+        return cuda_failure("cudaStreamIsCapturing", e);
+    }
+    if (capture == cudaStreamCaptureStatusNone) {
+        e = cudaStreamGetDevice(stream, &owner);
+        if (e != cudaSuccess) {
+            return cuda_failure("cudaStreamGetDevice", e);
+        }
+    } else {
+        owner = current;
     }
     return current == device && owner == device ? Status::success : Status::invalid_argument;
 }
@@ -597,7 +625,7 @@ Status build(const BatchRequest &request, PlanState &plan, cudaStream_t stream) 
     if (cudaGetDevice(&plan.device) != cudaSuccess ||
         cudaDeviceGetAttribute(&pageable, cudaDevAttrPageableMemoryAccess, plan.device) !=
             cudaSuccess) {
-        return cuda_failure();
+        return cuda_failure("cudaGetDevice/cudaDeviceGetAttribute");
     }
     plan.pageable = pageable != 0;
     st = stream_device(stream, plan.device);
@@ -637,7 +665,7 @@ Status build(const BatchRequest &request, PlanState &plan, cudaStream_t stream) 
     }
     if (cudaMallocAsync(&plan.storage, static_cast<std::size_t>(total), stream) != cudaSuccess) {
         plan.storage = nullptr;
-        return cuda_failure();
+        return cuda_failure("cudaMallocAsync (plan tables)");
     }
     auto *dev = static_cast<std::uint8_t *>(plan.storage);
     plan.images = reinterpret_cast<const tsk_decode_image *>(dev + at_images);
@@ -666,7 +694,7 @@ Status build(const BatchRequest &request, PlanState &plan, cudaStream_t stream) 
         break;
     }
     if (err != 0) {
-        return cuda_failure();
+        return cuda_failure("kernel preload", static_cast<cudaError_t>(err));
     }
     if (!upload(plan.storage, at_images, d.images, stream) ||
         !upload(plan.storage, at_tasks, d.tasks, stream) ||
@@ -675,7 +703,7 @@ Status build(const BatchRequest &request, PlanState &plan, cudaStream_t stream) 
         !upload(plan.storage, at_cal_images, d.calib_images, stream) ||
         !upload(plan.storage, at_cal_tasks, d.calib_tasks, stream) ||
         cudaStreamSynchronize(stream) != cudaSuccess) {
-        return cuda_failure();
+        return cuda_failure("plan table upload");
     }
     return Status::success;
 }
@@ -722,8 +750,12 @@ Status check_execution(const PlanState *plan, Operation operation, MutableBytes 
         st = accessible(results.data, plan->device, plan->pageable);
     }
     // A pending error from the caller's own work is left for the caller (docs/api.md:160).
-    if (st == Status::success && cudaPeekAtLastError() != cudaSuccess) {
-        st = Status::cuda_error;
+    if (st == Status::success) {
+        const cudaError_t pending = cudaPeekAtLastError();
+        if (pending != cudaSuccess) {
+            log_failure("pending error before enqueue (left for the caller)", pending);
+            st = Status::cuda_error;
+        }
     }
     return st;
 }
@@ -777,10 +809,11 @@ Status run_decode(const BatchPlan &plan, Operation op, MutableBytes workspace,
     auto *records = reinterpret_cast<tsk_result *>(results.data);
     if (p->trusted &&
         cudaMemsetAsync(records, 0, sizeof(tsk_result) * p->count, stream) != cudaSuccess) {
-        return detail::cuda_failure();
+        return detail::cuda_failure("cudaMemsetAsync (results)");
     }
     return detail::cuda_status(
-        tsk_decode_launch(p->tasks, p->task_count, p->images, p->rows, records, p->config, stream));
+        tsk_decode_launch(p->tasks, p->task_count, p->images, p->rows, records, p->config, stream),
+        "decode launch");
 }
 
 } // namespace
@@ -810,7 +843,7 @@ Status compress_async(const BatchPlan &plan, MutableBytes workspace, ResultBuffe
     void *state = static_cast<std::uint8_t *>(workspace.data) + p->layout.temp;
     return detail::cuda_status(tsk_encode_launch(
         p->encode_images, static_cast<std::uint32_t>(p->count), p->total_tiles, 0, state,
-        reinterpret_cast<tsk_result *>(results.data), stream));
+        reinterpret_cast<tsk_result *>(results.data), stream), "encode launch");
 }
 
 Status calibrate_async(const BatchPlan &plan, MutableBytes workspace, ResultBuffer results,
@@ -822,7 +855,7 @@ Status calibrate_async(const BatchPlan &plan, MutableBytes workspace, ResultBuff
     }
     return detail::cuda_status(tsk_calibrate_launch(
         p->calib_tasks, p->calib_task_count, p->calib_images, static_cast<std::uint32_t>(p->count),
-        reinterpret_cast<tsk_result *>(results.data), stream));
+        reinterpret_cast<tsk_result *>(results.data), stream), "calibrate launch");
 }
 
 } // namespace tilestream::cuda

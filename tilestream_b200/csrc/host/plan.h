@@ -34,19 +34,24 @@ inline Range range_of(const void *data, std::uint64_t size) noexcept {
     return {b, b + static_cast<std::uintptr_t>(size)};
 }
 
+// Writes "tilestream: <what> failed: <error>" to stderr when TILESTREAM_DEBUG is set.
+void log_failure(const char *what, cudaError_t error) noexcept;
+
 // A CUDA failure is reported through Status; the error is cleared so a later check cannot
 // blame it on another launch (reference plan.h:84-91).
-inline Status cuda_failure() noexcept {
-    static_cast<void>(cudaGetLastError());
+inline Status cuda_failure(const char *what = "CUDA runtime call",
+                           cudaError_t error = cudaErrorUnknown) noexcept {
+    const cudaError_t last = cudaGetLastError();
+    log_failure(what, error != cudaErrorUnknown ? error : last);
     return Status::cuda_error;
 }
 
-inline Status cuda_status(cudaError_t e) noexcept {
-    return e == cudaSuccess ? Status::success : cuda_failure();
+inline Status cuda_status(cudaError_t e, const char *what = "CUDA runtime call") noexcept {
+    return e == cudaSuccess ? Status::success : cuda_failure(what, e);
 }
 
-inline Status cuda_status(int e) noexcept {
-    return cuda_status(static_cast<cudaError_t>(e));
+inline Status cuda_status(int e, const char *what = "CUDA runtime call") noexcept {
+    return cuda_status(static_cast<cudaError_t>(e), what);
 }
 
 [[nodiscard]] Status accessible(const void *data, int device, bool pageable) noexcept;
