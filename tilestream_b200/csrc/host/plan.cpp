@@ -689,7 +689,11 @@ Status build(const BatchRequest &request, PlanState &plan, cudaStream_t stream) 
         err = tsk_calibrate_prepare(plan.device);
         break;
     default:
-        plan.config.group = 4;
+        // One pixel type per reference batch; the calibrated operation is the fused path.
+        plan.config.paths =
+            (d.type == PixelType::float32 ? TSK_PATH_F32 : TSK_PATH_U16) |
+            (request.operation == Operation::decode_calibrate ? TSK_PATH_CALIBRATED
+                                                              : TSK_PATH_PLAIN);
         err = tsk_decode_prepare(&plan.config, plan.task_count, plan.device);
         break;
     }

@@ -10,14 +10,16 @@
 //    stage through a second mbarrier. Payload offsets are only 4-byte aligned
 //    (docs/format.md:44), so the stage base is shifted by (src & 15) to keep the bulk part
 //    aligned on both sides.
-//  * warps 0-7 (consumers) decode rows. Each lane owns G consecutive columns: it extracts its
-//    residuals from shared-memory words with funnel shifts, undoes the transform (inverse
-//    zigzag mod 2^16 for uint16, XOR for FP32 words), scans them in registers, and a segmented
-//    warp-shuffle scan over the lanes of the row adds the totals of the groups to its left
-//    (decoder.cu:119-173 does the same per row with a lane-sequential group).
+//  * warps 0-7 (consumers) decode rows. A row is owned by LW lanes (a compile-time width class:
+//    the row's columns divided by G); each lane owns G consecutive columns. It loads a 64-bit
+//    window of the packed words per group of residuals, extracts them with funnel shifts, undoes
+//    the transform (inverse zigzag modulo 2^16 for uint16, XOR for FP32 words) and scans them in
+//    registers; an unrolled segmented warp-shuffle scan over the LW lanes adds the totals of the
+//    groups to the left, with the row seed as the initial carry (decoder.cu:119-173 does the
+//    same per row with a lane-sequential group and a 5-step scan).
 //  * RAW and CONSTANT tiles, ROI clipping (prediction still starts at column 0, decoder.cu:247),
 //    fused calibration RN(RN(x - offset) * gain) with __fsub_rn/__fmul_rn (device.cuh:81-85),
-//    vector stores when a group is aligned, and the trusted encoder-output path (index entry and
+//    16-byte stores when a group is aligned, and the trusted encoder-output path (index entry and
 //    row walk on the device, decoder.cu:86-110,191-220) all live in the same kernel.
 //
 // Results: a parsed image cannot fail on the device, so the first task of each image writes its
@@ -37,8 +39,6 @@ constexpr uint32_t kConsumerWarps = 8;
 constexpr uint32_t kConsumers = kConsumerWarps * 32;
 constexpr uint32_t kThreads = kConsumers + 32;
 constexpr uint32_t kFull = 0xffffffffu;
-// A payload stage: the largest tile plus alignment shift and over-read slack.
-constexpr uint32_t kStagePayload = TSK_PAYLOAD_BYTES + 128;
 
 enum : uint32_t { kStageOk = 0, kStageSkip = 1, kStageMalformed = 2 };
 
@@ -50,8 +50,11 @@ struct StageHeader {
     uint32_t state; // kStageOk / kStageSkip / kStageMalformed
 };
 
-template <uint32_t Stages> struct Shared {
-    alignas(128) uint8_t payload[Stages][kStagePayload];
+// MaxPayload: the largest tile payload of the plan (8 KiB for uint16-only plans, 16 KiB with
+// FP32). Each stage adds alignment shift and over-read slack.
+template <uint32_t MaxPayload, uint32_t Stages> struct Shared {
+    static constexpr uint32_t kStage = MaxPayload + 128;
+    alignas(128) uint8_t payload[Stages][kStage];
     alignas(16) uint16_t rows[Stages][TSK_MAX_ROWS];
     alignas(16) StageHeader header[Stages];
     alignas(8) uint64_t full[Stages];
@@ -60,20 +63,10 @@ template <uint32_t Stages> struct Shared {
 };
 
 // Paths compiled into one kernel instance.
-enum : uint32_t { kU16 = 1, kF32 = 2, kPlain = 4, kCal = 8, kTrusted = 16 };
+enum : uint32_t { kU16 = 1, kF32 = 2, kPlain = 4, kCal = 8 };
 
 __device__ __forceinline__ uint32_t low_mask(uint32_t bits) {
     return bits >= 32 ? 0xffffffffu : ((1u << bits) - 1u);
-}
-
-// Residual term of the inclusive scan (docs/format.md:81-97). uint16: the inverse zigzag as an
-// unsigned delta, s = z/2 or -(z/2) - 1, modulo 2^32 (narrowed to 16 bits at the end).
-template <bool F32> __device__ __forceinline__ uint32_t term(uint32_t z) {
-    if constexpr (F32) {
-        return z;
-    } else {
-        return (z >> 1) ^ (0u - (z & 1u));
-    }
 }
 
 template <bool F32> __device__ __forceinline__ uint32_t combine(uint32_t a, uint32_t b) {
@@ -92,129 +85,176 @@ template <bool F32> __device__ __forceinline__ uint32_t uncombine(uint32_t a, ui
     }
 }
 
-// Four residuals of at most 16 bits starting at bit pos of the row's packed words: one 64-bit
-// window (three shared loads) and funnel shifts, never a shift by 32 (docs/format.md:79).
-__device__ __forceinline__ void extract4(const uint32_t *w, uint32_t pos, uint32_t b, uint32_t m,
-                                         uint32_t r[4]) {
-    const uint32_t q = pos >> 5, s = pos & 31u;
-    const uint32_t w0 = w[q], w1 = w[q + 1], w2 = w[q + 2];
-    const uint32_t x0 = __funnelshift_r(w0, w1, s);
-    const uint32_t x1 = __funnelshift_r(w1, w2, s);
-    r[0] = x0 & m;
-    r[1] = __funnelshift_rc(x0, x1, b) & m;
-    const uint32_t y0 = __funnelshift_rc(x0, x1, 2 * b);
-    const uint32_t y1 = __funnelshift_rc(x1, 0u, 2 * b);
-    r[2] = y0 & m;
-    r[3] = __funnelshift_rc(y0, y1, b) & m;
-}
+// Per-task state in registers: output and calibration-map addresses of tile column 0 of the
+// first written row (these may lie before the region when the ROI starts inside the tile; they
+// are only dereferenced at columns inside it).
+struct Ctx {
+    uint8_t *out;
+    uint64_t pitch;
+    const uint8_t *omap;
+    uint64_t opitch;
+    const uint8_t *gmap;
+    uint64_t gpitch;
+    float offset, gain;
+    uint32_t w, row0, row1, col0, col1;
+};
 
-// Two residuals of up to 32 bits starting at bit pos.
-__device__ __forceinline__ void extract2(const uint32_t *w, uint32_t pos, uint32_t b, uint32_t m,
-                                         uint32_t r[2]) {
-    const uint32_t q = pos >> 5, s = pos & 31u;
-    const uint32_t w0 = w[q], w1 = w[q + 1], w2 = w[q + 2];
-    const uint32_t x0 = __funnelshift_r(w0, w1, s);
-    const uint32_t x1 = __funnelshift_r(w1, w2, s);
-    r[0] = x0 & m;
-    r[1] = __funnelshift_rc(x0, x1, b) & m;
-}
-
-// Calibration parameter for output pixel (x, y) (maps are in output-region coordinates).
-__device__ __forceinline__ float param(uint64_t map, uint64_t pitch, float scalar, uint64_t x,
-                                       uint64_t y) {
-    if (map == 0) {
-        return scalar;
+// Keeps only the first nbits bits of the 64-bit window (x1:x0); used for the lanes whose group
+// runs past the end of a partial row.
+__device__ __forceinline__ void keep_bits(uint32_t &x0, uint32_t &x1, uint32_t nbits) {
+    if (nbits < 32) {
+        x0 &= (1u << nbits) - 1u;
+        x1 = 0;
+    } else if (nbits < 64) {
+        x1 &= (1u << (nbits - 32)) - 1u;
     }
-    return reinterpret_cast<const float *>(map + y * pitch)[x];
 }
 
-__device__ __forceinline__ float sample_to_float(uint32_t v, bool f32) {
-    return f32 ? __uint_as_float(v) : static_cast<float>(v);
-}
-
-// Writes the G decoded values of one lane group: columns [c0, c0 + G) of tile row r.
-template <uint32_t G, bool F32, bool Cal>
-__device__ __forceinline__ void store_group(const tsk_decode_task &t, const tsk_decode_image &im,
-                                            uint32_t r, uint32_t c0, const uint32_t (&v)[G]) {
-    const uint32_t col0 = t.col0, col1 = t.col1;
-    if (c0 >= col1 || c0 + G <= col0) {
-        return;
+// The 64-bit window of the packed words that starts at the bit of item `first` of a row: item
+// c holds residual c - 1, item 0 holds zero (the seed is the scan's initial carry).
+__device__ __forceinline__ void window(const uint32_t *packed, uint32_t first, uint32_t b,
+                                       uint32_t &x0, uint32_t &x1) {
+    const int32_t pos = static_cast<int32_t>(first * b) - static_cast<int32_t>(b);
+    const uint32_t p = pos < 0 ? 0u : static_cast<uint32_t>(pos);
+    const uint32_t q = p >> 5, s = p & 31u;
+    const uint32_t w0 = packed[q], w1 = packed[q + 1], w2 = packed[q + 2];
+    x0 = __funnelshift_r(w0, w1, s);
+    x1 = __funnelshift_r(w1, w2, s);
+    if (pos < 0) {
+        // Item 0 of the row: shift a zero item in front of residual 0.
+        x1 = __funnelshift_lc(x0, x1, b);
+        x0 = __funnelshift_lc(0u, x0, b);
     }
-    const uint64_t oy = static_cast<uint64_t>(t.oy) + (r - t.row0);
-    // Output column of tile column c0 (may precede the region when c0 < col0).
-    const int64_t ox = static_cast<int64_t>(t.ox) + static_cast<int64_t>(c0) - col0;
-    if constexpr (Cal) {
-        float f[G];
-        const bool whole = c0 >= col0 && c0 + G <= col1;
+}
+
+// G scan terms of one lane: columns [c0, c0 + G) of a row of width w with residual width b.
+template <uint32_t G, bool F32>
+__device__ __forceinline__ void terms(const uint32_t *packed, uint32_t c0, uint32_t w, uint32_t b,
+                                      uint32_t (&t)[G]) {
+    if constexpr (!F32) {
+        // uint16, b <= 16: four residuals per 64-bit window.
+        const uint32_t mh = low_mask(b) >> 1;   // the magnitude bits of a zigzag value
+        const uint32_t sign = b != 0 ? 1u : 0u; // its sign bit (none when b = 0)
 #pragma unroll
-        for (uint32_t k = 0; k < G; ++k) {
-            const uint32_t c = c0 + k;
-            if (c >= col0 && c < col1) {
-                const uint64_t x = static_cast<uint64_t>(ox + k);
-                const float value = sample_to_float(v[k], F32);
-                f[k] = __fmul_rn(__fsub_rn(value, param(im.offset_map, im.offset_pitch, im.offset,
-                                                        x, oy)),
-                                 param(im.gain_map, im.gain_pitch, im.gain, x, oy));
-            } else {
-                f[k] = 0.0f;
+        for (uint32_t q = 0; q < G; q += 4) {
+            uint32_t x0, x1;
+            window(packed, c0 + q, b, x0, x1);
+            if (c0 + q + 4 > w) {
+                const uint32_t items = w > c0 + q ? w - (c0 + q) : 0u;
+                keep_bits(x0, x1, items * b);
+            }
+            uint32_t z[4];
+            z[0] = x0;
+            z[1] = __funnelshift_rc(x0, x1, b);
+            const uint32_t y0 = __funnelshift_rc(x0, x1, 2 * b);
+            const uint32_t y1 = __funnelshift_rc(x1, 0u, 2 * b);
+            z[2] = y0;
+            z[3] = __funnelshift_rc(y0, y1, b);
+#pragma unroll
+            for (uint32_t k = 0; k < 4; ++k) {
+                // Inverse zigzag as an unsigned delta: z/2 or -(z/2) - 1, modulo 2^32.
+                t[q + k] = ((z[k] >> 1) & mh) ^ (0u - (z[k] & sign));
             }
         }
-        float *line = reinterpret_cast<float *>(im.out + oy * im.out_pitch);
-        float *dst = line + ox;
-        if (whole && (reinterpret_cast<uintptr_t>(dst) % (4 * G)) == 0) {
-            if constexpr (G == 4) {
-                *reinterpret_cast<float4 *>(dst) = make_float4(f[0], f[1], f[2], f[3]);
-            } else {
-                reinterpret_cast<float4 *>(dst)[0] = make_float4(f[0], f[1], f[2], f[3]);
-                reinterpret_cast<float4 *>(dst)[1] = make_float4(f[4], f[5], f[6], f[7]);
+    } else {
+        // FP32 words, b <= 32: two residuals per 64-bit window.
+        const uint32_t m = low_mask(b);
+#pragma unroll
+        for (uint32_t q = 0; q < G; q += 2) {
+            uint32_t x0, x1;
+            window(packed, c0 + q, b, x0, x1);
+            if (c0 + q + 2 > w) {
+                const uint32_t items = w > c0 + q ? w - (c0 + q) : 0u;
+                keep_bits(x0, x1, items * b);
+            }
+            t[q] = x0 & m;
+            t[q + 1] = __funnelshift_rc(x0, x1, b) & m;
+        }
+    }
+}
+
+__device__ __forceinline__ float cal(float x, float o, float g) {
+    return __fmul_rn(__fsub_rn(x, o), g);
+}
+
+// Writes the G values of one lane: tile columns [c0, c0 + G) of the row at `line` (address of
+// tile column 0). Values are uint16 samples (low halves), FP32 words, or calibrated from them.
+template <uint32_t G, bool F32, bool Cal>
+__device__ __forceinline__ void store(const Ctx &x, uint8_t *line, const uint8_t *orow,
+                                      const uint8_t *grow, uint32_t c0, const uint32_t (&v)[G]) {
+    if (c0 >= x.col1 || c0 + G <= x.col0) {
+        return;
+    }
+    const bool whole = c0 >= x.col0 && c0 + G <= x.col1;
+    if constexpr (Cal) {
+        float *dst = reinterpret_cast<float *>(line) + c0;
+        const float *om = reinterpret_cast<const float *>(orow) + c0;
+        const float *gm = reinterpret_cast<const float *>(grow) + c0;
+        const bool vec = whole && ((reinterpret_cast<uintptr_t>(dst) |
+                                    (orow ? reinterpret_cast<uintptr_t>(om) : 0) |
+                                    (grow ? reinterpret_cast<uintptr_t>(gm) : 0)) & 15u) == 0;
+        if (vec) {
+#pragma unroll
+            for (uint32_t k = 0; k < G; k += 4) {
+                float4 o = make_float4(x.offset, x.offset, x.offset, x.offset);
+                float4 g = make_float4(x.gain, x.gain, x.gain, x.gain);
+                if (orow) o = __ldg(reinterpret_cast<const float4 *>(om + k));
+                if (grow) g = __ldg(reinterpret_cast<const float4 *>(gm + k));
+                float4 r;
+                r.x = cal(F32 ? __uint_as_float(v[k]) : static_cast<float>(v[k] & 0xffffu), o.x, g.x);
+                r.y = cal(F32 ? __uint_as_float(v[k + 1]) : static_cast<float>(v[k + 1] & 0xffffu),
+                          o.y, g.y);
+                r.z = cal(F32 ? __uint_as_float(v[k + 2]) : static_cast<float>(v[k + 2] & 0xffffu),
+                          o.z, g.z);
+                r.w = cal(F32 ? __uint_as_float(v[k + 3]) : static_cast<float>(v[k + 3] & 0xffffu),
+                          o.w, g.w);
+                *reinterpret_cast<float4 *>(dst + k) = r;
             }
         } else {
 #pragma unroll
             for (uint32_t k = 0; k < G; ++k) {
                 const uint32_t c = c0 + k;
-                if (c >= col0 && c < col1) {
-                    dst[k] = f[k];
+                if (c >= x.col0 && c < x.col1) {
+                    const float value =
+                        F32 ? __uint_as_float(v[k]) : static_cast<float>(v[k] & 0xffffu);
+                    dst[k] = cal(value, orow ? om[k] : x.offset, grow ? gm[k] : x.gain);
                 }
             }
         }
     } else if constexpr (F32) {
-        uint32_t *dst = reinterpret_cast<uint32_t *>(im.out + oy * im.out_pitch) + ox;
-        const bool whole = c0 >= col0 && c0 + G <= col1;
-        if (whole && (reinterpret_cast<uintptr_t>(dst) % (4 * G)) == 0) {
-            if constexpr (G == 4) {
-                *reinterpret_cast<uint4 *>(dst) = make_uint4(v[0], v[1], v[2], v[3]);
-            } else {
-                reinterpret_cast<uint4 *>(dst)[0] = make_uint4(v[0], v[1], v[2], v[3]);
-                reinterpret_cast<uint4 *>(dst)[1] = make_uint4(v[4], v[5], v[6], v[7]);
+        uint32_t *dst = reinterpret_cast<uint32_t *>(line) + c0;
+        if (whole && (reinterpret_cast<uintptr_t>(dst) & 15u) == 0) {
+#pragma unroll
+            for (uint32_t k = 0; k < G; k += 4) {
+                *reinterpret_cast<uint4 *>(dst + k) = make_uint4(v[k], v[k + 1], v[k + 2], v[k + 3]);
             }
         } else {
 #pragma unroll
             for (uint32_t k = 0; k < G; ++k) {
                 const uint32_t c = c0 + k;
-                if (c >= col0 && c < col1) {
+                if (c >= x.col0 && c < x.col1) {
                     dst[k] = v[k];
                 }
             }
         }
     } else {
-        uint16_t *dst = reinterpret_cast<uint16_t *>(im.out + oy * im.out_pitch) + ox;
-        const bool whole = c0 >= col0 && c0 + G <= col1;
-        if (whole && (reinterpret_cast<uintptr_t>(dst) % (2 * G)) == 0) {
+        uint16_t *dst = reinterpret_cast<uint16_t *>(line) + c0;
+        if (whole && (reinterpret_cast<uintptr_t>(dst) & (2 * G - 1)) == 0) {
             uint32_t p[G / 2];
 #pragma unroll
             for (uint32_t k = 0; k < G / 2; ++k) {
-                p[k] = (v[2 * k] & 0xffffu) | (v[2 * k + 1] << 16);
+                p[k] = __byte_perm(v[2 * k], v[2 * k + 1], 0x5410);
             }
-            if constexpr (G == 4) {
-                *reinterpret_cast<uint2 *>(dst) = make_uint2(p[0], p[1]);
-            } else {
+            if constexpr (G == 8) {
                 *reinterpret_cast<uint4 *>(dst) = make_uint4(p[0], p[1], p[2], p[3]);
+            } else {
+                *reinterpret_cast<uint2 *>(dst) = make_uint2(p[0], p[1]);
             }
         } else {
 #pragma unroll
             for (uint32_t k = 0; k < G; ++k) {
                 const uint32_t c = c0 + k;
-                if (c >= col0 && c < col1) {
+                if (c >= x.col0 && c < x.col1) {
                     dst[k] = static_cast<uint16_t>(v[k]);
                 }
             }
@@ -222,112 +262,110 @@ __device__ __forceinline__ void store_group(const tsk_decode_task &t, const tsk_
     }
 }
 
-// Decodes the rows [row0, row1) of one staged tile with the 8 consumer warps.
-template <uint32_t G, bool F32, bool Cal>
-__device__ void decode_tile(const tsk_decode_task &t, const tsk_decode_image &im,
-                            const uint32_t *payload, const uint16_t *rows, uint32_t mode) {
+// Decodes rows [row0, row1) of one staged tile with the 8 consumer warps; LW lanes per row.
+template <uint32_t G, uint32_t LW, bool F32, bool Cal>
+__device__ void decode_rows(const Ctx &x, const uint32_t *payload, const uint16_t *rows,
+                            uint32_t mode) {
+    constexpr uint32_t kRowsPerWarp = 32 / LW;
+    constexpr uint32_t kSpan = G * LW;
     const uint32_t warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-    const uint32_t w = t.width;
-    // Lanes per row: the smallest power of two whose groups cover the row, at most a warp.
-    const uint32_t need = (w + G - 1) / G;
-    const uint32_t lw = need >= 32 ? 32 : (need <= 1 ? 1 : 1u << (32 - __clz(need - 1)));
-    const uint32_t per_warp = 32 / lw;
-    const uint32_t sub = lane & (lw - 1);
-    const uint32_t span = G * lw; // columns covered by one pass of a row's lanes
-    // Columns 0..col1 must be decoded for prediction; passes beyond col1 are skipped.
-    const uint32_t passes = (t.col1 + span - 1) / span;
-    const uint32_t first_row = t.row0 + warp * per_warp;
-    const uint32_t stride = kConsumerWarps * per_warp;
-
-    for (uint32_t base = first_row; base < t.row1; base += stride) {
-        const uint32_t r = base + lane / lw;
-        const bool live = r < t.row1;
+    const uint32_t sub = lane % LW;
+    const uint32_t w = x.w;
+    for (uint32_t base = x.row0 + warp * kRowsPerWarp; base < x.row1;
+         base += kConsumerWarps * kRowsPerWarp) {
+        const uint32_t r = base + lane / LW;
+        const bool live = r < x.row1;
+        const uint64_t line_off = static_cast<uint64_t>(live ? r - x.row0 : 0u);
+        uint8_t *line = x.out + line_off * x.pitch;
+        const uint8_t *orow = nullptr, *grow = nullptr;
+        if constexpr (Cal) {
+            orow = x.omap ? x.omap + line_off * x.opitch : nullptr;
+            grow = x.gmap ? x.gmap + line_off * x.gpitch : nullptr;
+        }
         if (mode == TSK_PREDICT) {
             const uint32_t *row = payload + (live ? rows[r] : 0u);
-            const uint32_t seed = row[0];
-            const uint32_t b = row[1] & 0xffu;
-            const uint32_t m = low_mask(b);
+            const uint32_t b = live ? (row[1] & 0xffu) : 0u;
             const uint32_t *packed = row + 2;
-            uint32_t carry = 0;
+            // The seed is the initial carry: value(c) = seed (+ or ^) the terms of items 0..c.
+            uint32_t carry = live ? row[0] : 0u;
+            const uint32_t passes = (x.col1 + kSpan - 1) / kSpan;
             for (uint32_t pass = 0; pass < passes; ++pass) {
-                const uint32_t c0 = pass * span + sub * G;
-                // Residual j belongs to column j + 1; the lane at column 0 starts with the seed.
-                const uint32_t j0 = c0 == 0 ? 0u : c0 - 1;
-                uint32_t res[G];
+                const uint32_t c0 = pass * kSpan + sub * G;
+                uint32_t t[G];
                 if (live && c0 < w) {
-                    if constexpr (F32) {
-#pragma unroll
-                        for (uint32_t k = 0; k < G; k += 2) {
-                            extract2(packed, (j0 + k) * b, b, m, res + k);
-                        }
-                    } else {
-#pragma unroll
-                        for (uint32_t k = 0; k < G; k += 4) {
-                            extract4(packed, (j0 + k) * b, b, m, res + k);
-                        }
-                    }
+                    terms<G, F32>(packed, c0, w, b, t);
                 } else {
 #pragma unroll
                     for (uint32_t k = 0; k < G; ++k) {
-                        res[k] = 0;
+                        t[k] = 0;
                     }
                 }
-                uint32_t prefix[G];
-                uint32_t total = 0;
 #pragma unroll
-                for (uint32_t k = 0; k < G; ++k) {
-                    const uint32_t c = c0 + k;
-                    uint32_t item;
-                    if (c0 == 0) {
-                        item = k == 0 ? seed : term<F32>(res[k - (k > 0 ? 1 : 0)]);
-                    } else {
-                        item = term<F32>(res[k]);
-                    }
-                    item = (live && c < w) ? item : 0u;
-                    total = combine<F32>(total, item);
-                    prefix[k] = total;
+                for (uint32_t k = 1; k < G; ++k) {
+                    t[k] = combine<F32>(t[k - 1], t[k]);
                 }
+                const uint32_t total = t[G - 1];
                 uint32_t inclusive = total;
-                for (uint32_t d = 1; d < lw; d <<= 1) {
-                    const uint32_t other = __shfl_up_sync(kFull, inclusive, d, lw);
+#pragma unroll
+                for (uint32_t d = 1; d < LW; d <<= 1) {
+                    const uint32_t other = __shfl_up_sync(kFull, inclusive, d, LW);
                     if (sub >= d) {
                         inclusive = combine<F32>(other, inclusive);
                     }
                 }
                 const uint32_t before = combine<F32>(carry, uncombine<F32>(inclusive, total));
-                carry = combine<F32>(carry, __shfl_sync(kFull, inclusive, lw - 1, lw));
+                carry = combine<F32>(carry, __shfl_sync(kFull, inclusive, LW - 1, LW));
                 if (live) {
                     uint32_t v[G];
 #pragma unroll
                     for (uint32_t k = 0; k < G; ++k) {
-                        v[k] = combine<F32>(before, prefix[k]);
-                        if constexpr (!F32) {
-                            v[k] &= 0xffffu;
-                        }
+                        v[k] = combine<F32>(before, t[k]);
                     }
-                    store_group<G, F32, Cal>(t, im, r, c0, v);
+                    store<G, F32, Cal>(x, line, orow, grow, c0, v);
                 }
             }
         } else if (live) {
-            const uint32_t first_pass = t.col0 / span;
-            for (uint32_t pass = first_pass; pass < passes; ++pass) {
-                const uint32_t c0 = pass * span + sub * G;
+            const uint32_t passes = (x.col1 + kSpan - 1) / kSpan;
+            for (uint32_t pass = x.col0 / kSpan; pass < passes; ++pass) {
+                const uint32_t c0 = pass * kSpan + sub * G;
                 if (c0 >= w) {
                     continue;
                 }
                 uint32_t v[G];
 #pragma unroll
                 for (uint32_t k = 0; k < G; ++k) {
-                    const uint32_t c = c0 + k;
-                    uint32_t value = payload[0];
+                    const uint32_t c = c0 + k < w ? c0 + k : w - 1;
                     if (mode == TSK_RAW) {
-                        const uint32_t index = r * w + (c < w ? c : w - 1);
-                        value = F32 ? payload[index] : (payload[index >> 1] >> ((index & 1u) * 16));
+                        const uint32_t index = r * w + c;
+                        v[k] = F32 ? payload[index]
+                                   : reinterpret_cast<const uint16_t *>(payload)[index];
+                    } else {
+                        v[k] = F32 ? payload[0] : (payload[0] & 0xffffu);
                     }
-                    v[k] = F32 ? value : (value & 0xffffu);
                 }
-                store_group<G, F32, Cal>(t, im, r, c0, v);
+                store<G, F32, Cal>(x, line, orow, grow, c0, v);
             }
+        }
+    }
+}
+
+// Width classes: uint16 rows take 8 columns per lane, FP32 rows 4.
+template <bool F32, bool Cal>
+__device__ __forceinline__ void decode_tile(const Ctx &x, const uint32_t *payload,
+                                            const uint16_t *rows, uint32_t mode) {
+    if constexpr (!F32) {
+        if (x.w > 128) {
+            decode_rows<8, 32, false, Cal>(x, payload, rows, mode);
+        } else if (x.w > 64) {
+            decode_rows<8, 16, false, Cal>(x, payload, rows, mode);
+        } else {
+            decode_rows<8, 8, false, Cal>(x, payload, rows, mode);
+        }
+    } else {
+        if (x.w > 64) {
+            decode_rows<4, 32, true, Cal>(x, payload, rows, mode);
+        } else {
+            decode_rows<4, 16, true, Cal>(x, payload, rows, mode);
         }
     }
 }
@@ -361,9 +399,9 @@ __device__ __forceinline__ void fail(tsk_result *results, uint32_t image, uint32
     atomicCAS(&results[image].status, 0u, status);
 }
 
-// Producer: stages task k of this CTA into stage s.
-template <uint32_t Stages>
-__device__ void stage_task(Shared<Stages> &sh, uint32_t s, const tsk_decode_task &t,
+// Producer: stages one task into stage s.
+template <typename Sh>
+__device__ void stage_task(Sh &sh, uint32_t s, const tsk_decode_task &t,
                            const tsk_decode_image *images, const tsk_row_start *rowtab) {
     StageHeader &h = sh.header[s];
     uint64_t src = t.src;
@@ -374,18 +412,15 @@ __device__ void stage_task(Shared<Stages> &sh, uint32_t s, const tsk_decode_task
         const tsk_decode_image &im = images[t.image];
         const volatile tsk_result *producer =
             reinterpret_cast<const volatile tsk_result *>(im.encoder_result);
-        tsk_result produced;
-        produced.status = producer->status;
-        produced.bytes_written = producer->bytes_written;
-        if (produced.status != 0) {
+        const uint32_t produced_status = producer->status;
+        const uint64_t produced_bytes = producer->bytes_written;
+        if (produced_status != 0) {
             state = kStageSkip;
         } else {
-            const uint64_t end = produced.bytes_written < im.capacity ? produced.bytes_written
-                                                                      : im.capacity;
-            const uint8_t *slot = reinterpret_cast<const uint8_t *>(t.src) + 64 +
-                                  32 * t.words_or_tile;
+            const uint64_t end = produced_bytes < im.capacity ? produced_bytes : im.capacity;
             // The archive is only 4-byte aligned: read the entry as 32-bit words.
-            const uint32_t *e = reinterpret_cast<const uint32_t *>(slot);
+            const uint32_t *e = reinterpret_cast<const uint32_t *>(t.src + 64 +
+                                                                   32 * t.words_or_tile);
             const uint32_t e0 = e[0], e1 = e[1];
             const uint64_t offset = e[2] | (static_cast<uint64_t>(e[3]) << 32);
             const uint64_t length = e[4] | (static_cast<uint64_t>(e[5]) << 32);
@@ -404,7 +439,6 @@ __device__ void stage_task(Shared<Stages> &sh, uint32_t s, const tsk_decode_task
         }
     }
     const uint32_t shift = static_cast<uint32_t>(src & 15u);
-    uint32_t tx = 0;
     if (state == kStageOk) {
         uint8_t *base = sh.payload[s] + shift; // payload word 0
         const uint64_t end = src + 4ull * words;
@@ -416,8 +450,7 @@ __device__ void stage_task(Shared<Stages> &sh, uint32_t s, const tsk_decode_task
             cp_async4(base + (p - src), reinterpret_cast<const void *>(p));
             async_words = true;
         }
-        const uint64_t tail_begin = b > a ? b : a;
-        for (uint64_t p = tail_begin; p < end; p += 4) {
+        for (uint64_t p = b > a ? b : a; p < end; p += 4) {
             cp_async4(base + (p - src), reinterpret_cast<const void *>(p));
             async_words = true;
         }
@@ -427,7 +460,7 @@ __device__ void stage_task(Shared<Stages> &sh, uint32_t s, const tsk_decode_task
         const uint32_t body = b > a ? static_cast<uint32_t>(b - a) : 0u;
         const bool parsed_rows = !(t.flags & TSK_TRUSTED) && mode == TSK_PREDICT;
         const uint32_t row_bytes = parsed_rows ? (t.height * 2u + 15u) & ~15u : 0u;
-        tx = body + row_bytes;
+        const uint32_t tx = body + row_bytes;
         if (tx != 0) {
             mbar_expect_tx(&sh.full[s], tx);
         }
@@ -446,13 +479,14 @@ __device__ void stage_task(Shared<Stages> &sh, uint32_t s, const tsk_decode_task
     mbar_arrive(&sh.full[s]);
 }
 
-template <uint32_t G, uint32_t Stages, uint32_t Paths>
+template <uint32_t MaxPayload, uint32_t Stages, uint32_t Paths>
 __global__ void __launch_bounds__(kThreads)
     decode_kernel(const tsk_decode_task *__restrict__ tasks, uint32_t ntasks,
                   const tsk_decode_image *__restrict__ images,
                   const tsk_row_start *__restrict__ rowtab, tsk_result *results) {
+    using Sh = Shared<MaxPayload, Stages>;
     extern __shared__ __align__(128) uint8_t smem_raw[];
-    Shared<Stages> &sh = *reinterpret_cast<Shared<Stages> *>(smem_raw);
+    Sh &sh = *reinterpret_cast<Sh *>(smem_raw);
     const uint32_t warp = threadIdx.x / 32, lane = threadIdx.x % 32;
     if (threadIdx.x == 0) {
         for (uint32_t s = 0; s < Stages; ++s) {
@@ -465,12 +499,11 @@ __global__ void __launch_bounds__(kThreads)
     const uint32_t mine = blockIdx.x < ntasks ? (ntasks - 1 - blockIdx.x) / gridDim.x + 1 : 0;
 
     if (warp == kConsumerWarps) {
-        // Producer warp: lane 0 issues everything.
+        // Producer warp: lane 0 issues everything. The next task record is loaded before
+        // waiting for a free stage, so its latency overlaps the consumers' work.
         if (lane != 0) {
             return;
         }
-        // The next task record is loaded before waiting for a free stage, so its latency
-        // overlaps the consumers' work.
         tsk_decode_task t{};
         if (mine != 0) {
             t = tasks[blockIdx.x];
@@ -484,7 +517,7 @@ __global__ void __launch_bounds__(kThreads)
             if (i >= Stages && !mbar_wait(&sh.empty[s], ((i / Stages) - 1) & 1u)) {
                 return; // consumers stopped; they have reported the timeout
             }
-            stage_task<Stages>(sh, s, t, images, rowtab);
+            stage_task(sh, s, t, images, rowtab);
             t = next;
         }
         return;
@@ -494,110 +527,146 @@ __global__ void __launch_bounds__(kThreads)
         const uint32_t s = i % Stages;
         if (!mbar_wait(&sh.full[s], (i / Stages) & 1u)) {
             if (threadIdx.x == 0) {
-                const tsk_decode_task &t = tasks[blockIdx.x + i * gridDim.x];
-                fail(results, t.image, 9u); // cuda_error: a staging wait ran out
+                fail(results, tasks[blockIdx.x + i * gridDim.x].image, 9u); // cuda_error
             }
             return;
         }
         const StageHeader &h = sh.header[s];
         const tsk_decode_task t = h.task;
-        const tsk_decode_image &im = images[t.image];
+        const uint32_t state = h.state, hmode = h.mode;
         const uint32_t *payload = reinterpret_cast<const uint32_t *>(sh.payload[s] + h.shift);
         const bool f32 = (t.flags & TSK_F32) != 0;
-        const bool cal = (t.flags & TSK_CALIBRATED) != 0;
-        bool ok = h.state == kStageOk;
-        const uint16_t *rows = sh.rows[s];
-        if constexpr ((Paths & kTrusted) != 0) {
-            if ((t.flags & TSK_TRUSTED) && ok && h.mode == TSK_PREDICT) {
-                if (threadIdx.x == 0) {
-                    sh.valid[s] = walk_rows(payload, h.words, t.width, t.height, f32, sh.rows[s]);
-                }
-                named_sync(1, kConsumers);
-                ok = sh.valid[s] != 0;
+        const bool calibrated = (t.flags & TSK_CALIBRATED) != 0;
+        const bool trusted = (t.flags & TSK_TRUSTED) != 0;
+        const tsk_decode_image *im = images + t.image;
+        bool ok = state == kStageOk;
+        if (trusted && ok && hmode == TSK_PREDICT) {
+            if (threadIdx.x == 0) {
+                sh.valid[s] = walk_rows(payload, h.words, t.width, t.height, f32, sh.rows[s]);
             }
+            named_sync(1, kConsumers);
+            ok = sh.valid[s] != 0;
         }
         if (ok) {
+            Ctx x;
+            const uint64_t esize = calibrated || f32 ? 4u : 2u;
+            const uint64_t pitch = im->out_pitch;
+            x.pitch = pitch;
+            x.out = reinterpret_cast<uint8_t *>(im->out) + t.oy * pitch +
+                    (static_cast<int64_t>(t.ox) - t.col0) * static_cast<int64_t>(esize);
+            x.w = t.width;
+            x.row0 = t.row0;
+            x.row1 = t.row1;
+            x.col0 = t.col0;
+            x.col1 = t.col1;
+            x.omap = x.gmap = nullptr;
+            x.opitch = x.gpitch = 0;
+            x.offset = 0.0f;
+            x.gain = 1.0f;
+            if (calibrated) {
+                const int64_t cx = static_cast<int64_t>(t.ox) - t.col0;
+                x.offset = im->offset;
+                x.gain = im->gain;
+                x.opitch = im->offset_pitch;
+                x.gpitch = im->gain_pitch;
+                if (im->offset_map) {
+                    x.omap = reinterpret_cast<const uint8_t *>(im->offset_map) + t.oy * x.opitch +
+                             cx * 4;
+                }
+                if (im->gain_map) {
+                    x.gmap = reinterpret_cast<const uint8_t *>(im->gain_map) + t.oy * x.gpitch +
+                             cx * 4;
+                }
+            }
+            const uint16_t *rows = sh.rows[s];
             if constexpr ((Paths & kU16) && (Paths & kPlain)) {
-                if (!f32 && !cal) decode_tile<G, false, false>(t, im, payload, rows, h.mode);
+                if (!f32 && !calibrated) decode_tile<false, false>(x, payload, rows, hmode);
             }
             if constexpr ((Paths & kF32) && (Paths & kPlain)) {
-                if (f32 && !cal) decode_tile<G, true, false>(t, im, payload, rows, h.mode);
+                if (f32 && !calibrated) decode_tile<true, false>(x, payload, rows, hmode);
             }
             if constexpr ((Paths & kU16) && (Paths & kCal)) {
-                if (!f32 && cal) decode_tile<G, false, true>(t, im, payload, rows, h.mode);
+                if (!f32 && calibrated) decode_tile<false, true>(x, payload, rows, hmode);
             }
             if constexpr ((Paths & kF32) && (Paths & kCal)) {
-                if (f32 && cal) decode_tile<G, true, true>(t, im, payload, rows, h.mode);
+                if (f32 && calibrated) decode_tile<true, true>(x, payload, rows, hmode);
             }
-        }
-        if ((t.flags & TSK_TRUSTED) && threadIdx.x == 0 && h.state == kStageMalformed) {
-            fail(results, t.image, 5u); // malformed_data
-        }
-        if ((t.flags & TSK_TRUSTED) && threadIdx.x == 0 && h.state == kStageOk && !ok) {
-            fail(results, t.image, 5u);
         }
         __syncwarp();
         if (lane == 0) {
             mbar_arrive(&sh.empty[s]);
         }
         if (threadIdx.x == 0) {
-            if (t.flags & TSK_TRUSTED) {
+            if (trusted) {
+                if (state == kStageMalformed || (state == kStageOk && !ok)) {
+                    fail(results, t.image, 5u); // malformed_data
+                }
                 // Completion count: the last task of the image writes the final record.
                 __threadfence();
                 const uint32_t done = atomicAdd(&results[t.image].reserved, 1u);
-                if (done + 1 == im.tile_count) {
+                if (done + 1 == im->tile_count) {
                     __threadfence();
-                    uint32_t status = *reinterpret_cast<volatile uint32_t *>(
-                        &results[t.image].status);
-                    const uint32_t produced = reinterpret_cast<const volatile tsk_result *>(
-                                                  im.encoder_result)
-                                                  ->status;
+                    uint32_t status =
+                        *reinterpret_cast<volatile uint32_t *>(&results[t.image].status);
+                    const uint32_t produced =
+                        reinterpret_cast<const volatile tsk_result *>(im->encoder_result)->status;
                     if (produced != 0) {
                         status = produced;
                     }
                     results[t.image].reserved = 0;
-                    results[t.image].bytes_written = status == 0 ? im.result_bytes : 0;
+                    results[t.image].bytes_written = status == 0 ? im->result_bytes : 0;
                     results[t.image].status = status;
                 }
             } else if (t.flags & TSK_FIRST) {
                 results[t.image].status = 0;
                 results[t.image].reserved = 0;
-                results[t.image].bytes_written = im.result_bytes;
+                results[t.image].bytes_written = im->result_bytes;
             }
         }
     }
 }
 
-template <uint32_t Stages> constexpr size_t smem_bytes() {
-    return sizeof(Shared<Stages>);
-}
-
 using KernelFn = void (*)(const tsk_decode_task *, uint32_t, const tsk_decode_image *,
                           const tsk_row_start *, tsk_result *);
 
-constexpr uint32_t kStages = 3;
-constexpr uint32_t kAll = kU16 | kF32 | kPlain | kCal | kTrusted;
+struct Variant {
+    KernelFn fn;
+    size_t smem;
+};
 
-template <uint32_t G> KernelFn kernel_for() {
-    return decode_kernel<G, kStages, kAll>;
+// Kernel instances: uint16-only plans stage 8 KiB tiles (four stages), plans with FP32 stage
+// 16 KiB tiles (three stages); the calibrated and plain paths are separate instances so that a
+// plan's kernel carries only the code (and registers) it needs.
+template <uint32_t MaxPayload, uint32_t Stages, uint32_t Paths> Variant make() {
+    return {decode_kernel<MaxPayload, Stages, Paths>, sizeof(Shared<MaxPayload, Stages>)};
 }
 
-KernelFn select(uint32_t group) {
-    return group == 8 ? kernel_for<8>() : kernel_for<4>();
+Variant select(uint32_t paths) {
+    const bool f32 = paths & kF32, u16 = paths & kU16, plain = paths & kPlain, c = paths & kCal;
+    if (!f32) {
+        if (plain && !c) return make<8192, 4, kU16 | kPlain>();
+        if (c && !plain) return make<8192, 4, kU16 | kCal>();
+        return make<8192, 4, kU16 | kPlain | kCal>();
+    }
+    if (!u16) {
+        if (plain && !c) return make<16384, 3, kF32 | kPlain>();
+        if (c && !plain) return make<16384, 3, kF32 | kCal>();
+    }
+    return make<16384, 3, kU16 | kF32 | kPlain | kCal>();
 }
 
 } // namespace
 } // namespace tsk
 
+// Sets the kernel instance's shared-memory limit (which also loads it) and fills in the
+// occupancy-derived persistent grid for the plan's path mask.
 extern "C" int tsk_decode_prepare(tsk_decode_config *config, uint32_t ntasks, int device) {
-    const uint32_t group = config->group == 8 ? 8u : 4u;
-    auto fn = tsk::select(group);
-    const size_t smem = tsk::smem_bytes<tsk::kStages>();
-    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(smem));
+    const tsk::Variant v = tsk::select(config->paths);
+    cudaError_t e = cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(v.smem));
     if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, tsk::kThreads, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v.fn, tsk::kThreads, v.smem);
     if (e != cudaSuccess) return e;
     int sms = 0;
     e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
@@ -607,8 +676,8 @@ extern "C" int tsk_decode_prepare(tsk_decode_config *config, uint32_t ntasks, in
     if (grid > ntasks) grid = ntasks;
     if (grid < 1) grid = 1;
     config->grid = static_cast<uint32_t>(grid);
-    config->group = group;
-    config->stages = tsk::kStages;
+    config->per_sm = static_cast<uint32_t>(per_sm);
+    config->smem = static_cast<uint32_t>(v.smem);
     return cudaSuccess;
 }
 
@@ -617,8 +686,7 @@ extern "C" int tsk_decode_launch(const tsk_decode_task *tasks, uint32_t ntasks,
                                  tsk_result *results, tsk_decode_config config,
                                  cudaStream_t stream) {
     if (ntasks == 0) return cudaSuccess;
-    auto fn = tsk::select(config.group);
-    const size_t smem = tsk::smem_bytes<tsk::kStages>();
-    fn<<<config.grid, tsk::kThreads, smem, stream>>>(tasks, ntasks, images, rows, results);
+    const tsk::Variant v = tsk::select(config.paths);
+    v.fn<<<config.grid, tsk::kThreads, v.smem, stream>>>(tasks, ntasks, images, rows, results);
     return cudaGetLastError();
 }

@@ -76,12 +76,21 @@ typedef struct __align__(16) {
 typedef uint16_t tsk_row_start;
 #define TSK_ROW_SLOT TSK_MAX_ROWS
 
-// Launch parameters chosen by the planner (and by the autotuner for batches).
+// Decode kernel paths a plan needs (tsk_decode_config.paths).
+enum {
+    TSK_PATH_U16 = 1,
+    TSK_PATH_F32 = 2,
+    TSK_PATH_PLAIN = 4,
+    TSK_PATH_CALIBRATED = 8,
+};
+
+// Launch parameters of a decode plan: `paths` is set by the planner, the rest by
+// tsk_decode_prepare (and may be lowered by the autotuner).
 typedef struct {
     uint32_t grid;   // persistent CTAs
-    uint32_t group;  // columns per lane: 4 or 8
-    uint32_t stages; // staging depth: 2 or 3 (fixed by the kernel build)
-    uint32_t reserved;
+    uint32_t per_sm; // resident CTAs per SM at the kernel's occupancy
+    uint32_t smem;   // dynamic shared memory per CTA in bytes
+    uint32_t paths;  // TSK_PATH_* mask selecting the kernel instance
 } tsk_decode_config;
 
 // One image to encode. 96 bytes.
