@@ -341,8 +341,11 @@ Status check_tile(const ImageMetadata &m, std::uint64_t index) noexcept {
 }
 
 // The ROI clip of one tile: rows [row0, row1) and columns [col0, col1) of the tile, placed at
-// output (ox, oy).
-void clip(tsk_decode_task &t, const Roi &roi, std::uint64_t x, std::uint64_t y) {
+// output (ox, oy); dst addresses tile column 0 of row row0 in the output. A tile whose rows are
+// written whole, have a width the decoder's lane groups cover exactly, and land on 16-byte
+// aligned output (and map) rows is marked TSK_FULL: the kernel then stores without checks.
+void clip(tsk_decode_task &t, const Roi &roi, std::uint64_t x, std::uint64_t y,
+          const tsk_decode_image &im, bool calibrated, std::uint64_t sample) {
     const std::uint64_t rx1 = std::uint64_t{roi.x} + roi.width;
     const std::uint64_t ry1 = std::uint64_t{roi.y} + roi.height;
     t.row0 = static_cast<std::uint16_t>(roi.y > y ? roi.y - y : 0);
@@ -351,13 +354,33 @@ void clip(tsk_decode_task &t, const Roi &roi, std::uint64_t x, std::uint64_t y) 
     t.col1 = static_cast<std::uint16_t>(rx1 < x + t.width ? rx1 - x : t.width);
     t.ox = static_cast<std::uint32_t>(x + t.col0 - roi.x);
     t.oy = static_cast<std::uint32_t>(y + t.row0 - roi.y);
+    const std::uint64_t esize = calibrated ? 4 : sample;
+    // Unsigned wrap-around gives the address before the region when t.ox < t.col0.
+    t.dst = im.out + t.oy * im.out_pitch + (std::uint64_t{t.ox} - t.col0) * esize;
+    t.pitch = im.out_pitch;
+    const bool class_width = t.width == 64 || t.width == 128 || t.width == 256;
+    bool aligned = ((t.dst | t.pitch) & 15u) == 0;
+    if (calibrated) {
+        for (const auto &[map, pitch] : {std::pair{im.offset_map, im.offset_pitch},
+                                         std::pair{im.gain_map, im.gain_pitch}}) {
+            if (map != 0) {
+                aligned = aligned && (((map + t.oy * pitch + std::uint64_t{t.ox} * 4) | pitch) &
+                                      15u) == 0;
+            }
+        }
+    }
+    if (class_width && t.col0 == 0 && t.col1 == t.width && aligned) {
+        t.flags |= TSK_FULL;
+    }
 }
 
 // Selects the tiles that intersect the region (row-major) and rebases them into the supplied
 // bytes (reference plan.cpp:281-349).
 Status stage_tiles(const CompressedInput &src, const Roi &roi, std::uint32_t image,
-                   std::uint8_t flags, Draft &d) {
+                   std::uint8_t flags, const tsk_decode_image &rec, Draft &d) {
     const ImageMetadata &m = *src.metadata;
+    const bool calibrated = (flags & TSK_CALIBRATED) != 0;
+    const std::uint64_t sample = m.image.type == PixelType::uint16 ? 2 : 4;
     const std::uint64_t across = tiles_across(m.image, m.tile);
     if (m.tiles.size() != across * tiles_down(m.image, m.tile)) {
         return Status::malformed_data;
@@ -403,7 +426,7 @@ Status stage_tiles(const CompressedInput &src, const Roi &roi, std::uint32_t ima
             task.height = t.height;
             task.mode = static_cast<std::uint8_t>(t.mode);
             task.flags = flags | (k == 0 ? TSK_FIRST : 0);
-            clip(task, roi, col * m.tile.width, row * m.tile.height);
+            clip(task, roi, col * m.tile.width, row * m.tile.height, rec, calibrated, sample);
             if (t.mode == TileMode::predict_bitpack) {
                 task.rows_at = static_cast<std::uint32_t>(d.rows.size());
                 d.rows.resize(d.rows.size() + TSK_ROW_SLOT, 0);
@@ -529,7 +552,8 @@ Status draft_decode(const BatchRequest &request, Draft &d) {
                     task.height = static_cast<std::uint16_t>(
                         std::min<std::uint64_t>(shape.height, image.height - y));
                     task.flags = flags | TSK_TRUSTED;
-                    clip(task, roi, x, y);
+                    clip(task, roi, x, y, rec, calibrated,
+                         image.type == PixelType::uint16 ? 2 : 4);
                     d.tasks.push_back(task);
                 }
             }
@@ -540,7 +564,7 @@ Status draft_decode(const BatchRequest &request, Draft &d) {
             d.readable.push_back(range_of(src.encoder_result, sizeof(DeviceResult)));
             d.pointers.push_back(src.encoder_result);
         } else {
-            st = stage_tiles(src, roi, index, flags, d);
+            st = stage_tiles(src, roi, index, flags, rec, d);
             if (st != Status::success) {
                 return st;
             }

@@ -42,8 +42,13 @@ constexpr uint32_t kFull = 0xffffffffu;
 
 enum : uint32_t { kStageOk = 0, kStageSkip = 1, kStageMalformed = 2 };
 
+// Everything the consumers need about one staged tile, written by the producer.
 struct StageHeader {
     tsk_decode_task task;
+    // Calibrated tiles: map addresses of tile column 0 in row row0 (0 for a scalar parameter).
+    uint64_t omap, gmap;
+    uint64_t opitch, gpitch;
+    float offset, gain;
     uint32_t shift; // byte offset of payload word 0 within the stage buffer
     uint32_t words; // payload words
     uint32_t mode;
@@ -97,6 +102,7 @@ struct Ctx {
     uint64_t gpitch;
     float offset, gain;
     uint32_t w, row0, row1, col0, col1;
+    bool full; // TSK_FULL: whole rows of a class width, 16-byte-aligned rows
 };
 
 // Keeps only the first nbits bits of the 64-bit window (x1:x0); used for the lanes whose group
@@ -128,7 +134,8 @@ __device__ __forceinline__ void window(const uint32_t *packed, uint32_t first, u
 }
 
 // G scan terms of one lane: columns [c0, c0 + G) of a row of width w with residual width b.
-template <uint32_t G, bool F32>
+// Partial: the group may run past the end of the row (those items become zero).
+template <uint32_t G, bool F32, bool Partial>
 __device__ __forceinline__ void terms(const uint32_t *packed, uint32_t c0, uint32_t w, uint32_t b,
                                       uint32_t (&t)[G]) {
     if constexpr (!F32) {
@@ -139,9 +146,11 @@ __device__ __forceinline__ void terms(const uint32_t *packed, uint32_t c0, uint3
         for (uint32_t q = 0; q < G; q += 4) {
             uint32_t x0, x1;
             window(packed, c0 + q, b, x0, x1);
-            if (c0 + q + 4 > w) {
-                const uint32_t items = w > c0 + q ? w - (c0 + q) : 0u;
-                keep_bits(x0, x1, items * b);
+            if constexpr (Partial) {
+                if (c0 + q + 4 > w) {
+                    const uint32_t items = w > c0 + q ? w - (c0 + q) : 0u;
+                    keep_bits(x0, x1, items * b);
+                }
             }
             uint32_t z[4];
             z[0] = x0;
@@ -163,9 +172,11 @@ __device__ __forceinline__ void terms(const uint32_t *packed, uint32_t c0, uint3
         for (uint32_t q = 0; q < G; q += 2) {
             uint32_t x0, x1;
             window(packed, c0 + q, b, x0, x1);
-            if (c0 + q + 2 > w) {
-                const uint32_t items = w > c0 + q ? w - (c0 + q) : 0u;
-                keep_bits(x0, x1, items * b);
+            if constexpr (Partial) {
+                if (c0 + q + 2 > w) {
+                    const uint32_t items = w > c0 + q ? w - (c0 + q) : 0u;
+                    keep_bits(x0, x1, items * b);
+                }
             }
             t[q] = x0 & m;
             t[q + 1] = __funnelshift_rc(x0, x1, b) & m;
@@ -177,22 +188,39 @@ __device__ __forceinline__ float cal(float x, float o, float g) {
     return __fmul_rn(__fsub_rn(x, o), g);
 }
 
+template <bool F32> __device__ __forceinline__ float as_value(uint32_t v) {
+    if constexpr (F32) {
+        return __uint_as_float(v);
+    } else {
+        return static_cast<float>(v & 0xffffu);
+    }
+}
+
 // Writes the G values of one lane: tile columns [c0, c0 + G) of the row at `line` (address of
 // tile column 0). Values are uint16 samples (low halves), FP32 words, or calibrated from them.
-template <uint32_t G, bool F32, bool Cal>
+// Full: the group is inside the written columns and every address is 16-byte aligned.
+template <uint32_t G, bool F32, bool Cal, bool Full>
 __device__ __forceinline__ void store(const Ctx &x, uint8_t *line, const uint8_t *orow,
                                       const uint8_t *grow, uint32_t c0, const uint32_t (&v)[G]) {
-    if (c0 >= x.col1 || c0 + G <= x.col0) {
-        return;
+    if constexpr (!Full) {
+        if (c0 >= x.col1 || c0 + G <= x.col0) {
+            return;
+        }
     }
-    const bool whole = c0 >= x.col0 && c0 + G <= x.col1;
+    bool whole = true;
+    if constexpr (!Full) {
+        whole = c0 >= x.col0 && c0 + G <= x.col1;
+    }
     if constexpr (Cal) {
         float *dst = reinterpret_cast<float *>(line) + c0;
         const float *om = reinterpret_cast<const float *>(orow) + c0;
         const float *gm = reinterpret_cast<const float *>(grow) + c0;
-        const bool vec = whole && ((reinterpret_cast<uintptr_t>(dst) |
-                                    (orow ? reinterpret_cast<uintptr_t>(om) : 0) |
-                                    (grow ? reinterpret_cast<uintptr_t>(gm) : 0)) & 15u) == 0;
+        bool vec = true;
+        if constexpr (!Full) {
+            vec = whole && ((reinterpret_cast<uintptr_t>(dst) |
+                             (orow ? reinterpret_cast<uintptr_t>(om) : 0) |
+                             (grow ? reinterpret_cast<uintptr_t>(gm) : 0)) & 15u) == 0;
+        }
         if (vec) {
 #pragma unroll
             for (uint32_t k = 0; k < G; k += 4) {
@@ -201,13 +229,10 @@ __device__ __forceinline__ void store(const Ctx &x, uint8_t *line, const uint8_t
                 if (orow) o = __ldg(reinterpret_cast<const float4 *>(om + k));
                 if (grow) g = __ldg(reinterpret_cast<const float4 *>(gm + k));
                 float4 r;
-                r.x = cal(F32 ? __uint_as_float(v[k]) : static_cast<float>(v[k] & 0xffffu), o.x, g.x);
-                r.y = cal(F32 ? __uint_as_float(v[k + 1]) : static_cast<float>(v[k + 1] & 0xffffu),
-                          o.y, g.y);
-                r.z = cal(F32 ? __uint_as_float(v[k + 2]) : static_cast<float>(v[k + 2] & 0xffffu),
-                          o.z, g.z);
-                r.w = cal(F32 ? __uint_as_float(v[k + 3]) : static_cast<float>(v[k + 3] & 0xffffu),
-                          o.w, g.w);
+                r.x = cal(as_value<F32>(v[k]), o.x, g.x);
+                r.y = cal(as_value<F32>(v[k + 1]), o.y, g.y);
+                r.z = cal(as_value<F32>(v[k + 2]), o.z, g.z);
+                r.w = cal(as_value<F32>(v[k + 3]), o.w, g.w);
                 *reinterpret_cast<float4 *>(dst + k) = r;
             }
         } else {
@@ -215,15 +240,14 @@ __device__ __forceinline__ void store(const Ctx &x, uint8_t *line, const uint8_t
             for (uint32_t k = 0; k < G; ++k) {
                 const uint32_t c = c0 + k;
                 if (c >= x.col0 && c < x.col1) {
-                    const float value =
-                        F32 ? __uint_as_float(v[k]) : static_cast<float>(v[k] & 0xffffu);
-                    dst[k] = cal(value, orow ? om[k] : x.offset, grow ? gm[k] : x.gain);
+                    dst[k] = cal(as_value<F32>(v[k]), orow ? om[k] : x.offset,
+                                 grow ? gm[k] : x.gain);
                 }
             }
         }
     } else if constexpr (F32) {
         uint32_t *dst = reinterpret_cast<uint32_t *>(line) + c0;
-        if (whole && (reinterpret_cast<uintptr_t>(dst) & 15u) == 0) {
+        if (Full || (whole && (reinterpret_cast<uintptr_t>(dst) & 15u) == 0)) {
 #pragma unroll
             for (uint32_t k = 0; k < G; k += 4) {
                 *reinterpret_cast<uint4 *>(dst + k) = make_uint4(v[k], v[k + 1], v[k + 2], v[k + 3]);
@@ -239,7 +263,7 @@ __device__ __forceinline__ void store(const Ctx &x, uint8_t *line, const uint8_t
         }
     } else {
         uint16_t *dst = reinterpret_cast<uint16_t *>(line) + c0;
-        if (whole && (reinterpret_cast<uintptr_t>(dst) & (2 * G - 1)) == 0) {
+        if (Full || (whole && (reinterpret_cast<uintptr_t>(dst) & (2 * G - 1)) == 0)) {
             uint32_t p[G / 2];
 #pragma unroll
             for (uint32_t k = 0; k < G / 2; ++k) {
@@ -263,7 +287,9 @@ __device__ __forceinline__ void store(const Ctx &x, uint8_t *line, const uint8_t
 }
 
 // Decodes rows [row0, row1) of one staged tile with the 8 consumer warps; LW lanes per row.
-template <uint32_t G, uint32_t LW, bool F32, bool Cal>
+// Full: the tile's width is G * LW (or twice that for FP32 256-wide rows) and every column is
+// written to aligned rows, so no per-group bounds or alignment checks are needed.
+template <uint32_t G, uint32_t LW, bool F32, bool Cal, bool Full>
 __device__ void decode_rows(const Ctx &x, const uint32_t *payload, const uint16_t *rows,
                             uint32_t mode) {
     constexpr uint32_t kRowsPerWarp = 32 / LW;
@@ -271,6 +297,7 @@ __device__ void decode_rows(const Ctx &x, const uint32_t *payload, const uint16_
     const uint32_t warp = threadIdx.x / 32, lane = threadIdx.x % 32;
     const uint32_t sub = lane % LW;
     const uint32_t w = x.w;
+    const uint32_t passes = (x.col1 + kSpan - 1) / kSpan;
     for (uint32_t base = x.row0 + warp * kRowsPerWarp; base < x.row1;
          base += kConsumerWarps * kRowsPerWarp) {
         const uint32_t r = base + lane / LW;
@@ -288,12 +315,11 @@ __device__ void decode_rows(const Ctx &x, const uint32_t *payload, const uint16_
             const uint32_t *packed = row + 2;
             // The seed is the initial carry: value(c) = seed (+ or ^) the terms of items 0..c.
             uint32_t carry = live ? row[0] : 0u;
-            const uint32_t passes = (x.col1 + kSpan - 1) / kSpan;
             for (uint32_t pass = 0; pass < passes; ++pass) {
                 const uint32_t c0 = pass * kSpan + sub * G;
                 uint32_t t[G];
-                if (live && c0 < w) {
-                    terms<G, F32>(packed, c0, w, b, t);
+                if (Full || c0 < w) {
+                    terms<G, F32, !Full>(packed, c0, w, b, t);
                 } else {
 #pragma unroll
                     for (uint32_t k = 0; k < G; ++k) {
@@ -321,20 +347,19 @@ __device__ void decode_rows(const Ctx &x, const uint32_t *payload, const uint16_
                     for (uint32_t k = 0; k < G; ++k) {
                         v[k] = combine<F32>(before, t[k]);
                     }
-                    store<G, F32, Cal>(x, line, orow, grow, c0, v);
+                    store<G, F32, Cal, Full>(x, line, orow, grow, c0, v);
                 }
             }
         } else if (live) {
-            const uint32_t passes = (x.col1 + kSpan - 1) / kSpan;
             for (uint32_t pass = x.col0 / kSpan; pass < passes; ++pass) {
                 const uint32_t c0 = pass * kSpan + sub * G;
-                if (c0 >= w) {
+                if (!Full && c0 >= w) {
                     continue;
                 }
                 uint32_t v[G];
 #pragma unroll
                 for (uint32_t k = 0; k < G; ++k) {
-                    const uint32_t c = c0 + k < w ? c0 + k : w - 1;
+                    const uint32_t c = Full || c0 + k < w ? c0 + k : w - 1;
                     if (mode == TSK_RAW) {
                         const uint32_t index = r * w + c;
                         v[k] = F32 ? payload[index]
@@ -343,9 +368,19 @@ __device__ void decode_rows(const Ctx &x, const uint32_t *payload, const uint16_
                         v[k] = F32 ? payload[0] : (payload[0] & 0xffffu);
                     }
                 }
-                store<G, F32, Cal>(x, line, orow, grow, c0, v);
+                store<G, F32, Cal, Full>(x, line, orow, grow, c0, v);
             }
         }
+    }
+}
+
+template <uint32_t G, uint32_t LW, bool F32, bool Cal>
+__device__ __forceinline__ void decode_class(const Ctx &x, const uint32_t *payload,
+                                             const uint16_t *rows, uint32_t mode) {
+    if (x.full) {
+        decode_rows<G, LW, F32, Cal, true>(x, payload, rows, mode);
+    } else {
+        decode_rows<G, LW, F32, Cal, false>(x, payload, rows, mode);
     }
 }
 
@@ -355,17 +390,17 @@ __device__ __forceinline__ void decode_tile(const Ctx &x, const uint32_t *payloa
                                             const uint16_t *rows, uint32_t mode) {
     if constexpr (!F32) {
         if (x.w > 128) {
-            decode_rows<8, 32, false, Cal>(x, payload, rows, mode);
+            decode_class<8, 32, false, Cal>(x, payload, rows, mode);
         } else if (x.w > 64) {
-            decode_rows<8, 16, false, Cal>(x, payload, rows, mode);
+            decode_class<8, 16, false, Cal>(x, payload, rows, mode);
         } else {
-            decode_rows<8, 8, false, Cal>(x, payload, rows, mode);
+            decode_class<8, 8, false, Cal>(x, payload, rows, mode);
         }
     } else {
         if (x.w > 64) {
-            decode_rows<4, 32, true, Cal>(x, payload, rows, mode);
+            decode_class<4, 32, true, Cal>(x, payload, rows, mode);
         } else {
-            decode_rows<4, 16, true, Cal>(x, payload, rows, mode);
+            decode_class<4, 16, true, Cal>(x, payload, rows, mode);
         }
     }
 }
@@ -472,6 +507,16 @@ __device__ void stage_task(Sh &sh, uint32_t s, const tsk_decode_task &t,
         }
     }
     h.task = t;
+    if (t.flags & TSK_CALIBRATED) {
+        const tsk_decode_image &im = images[t.image];
+        const int64_t cx = static_cast<int64_t>(t.ox) - t.col0;
+        h.offset = im.offset;
+        h.gain = im.gain;
+        h.opitch = im.offset_pitch;
+        h.gpitch = im.gain_pitch;
+        h.omap = im.offset_map ? im.offset_map + t.oy * im.offset_pitch + cx * 4 : 0;
+        h.gmap = im.gain_map ? im.gain_map + t.oy * im.gain_pitch + cx * 4 : 0;
+    }
     h.shift = shift;
     h.words = words;
     h.mode = mode;
@@ -480,7 +525,9 @@ __device__ void stage_task(Sh &sh, uint32_t s, const tsk_decode_task &t,
 }
 
 template <uint32_t MaxPayload, uint32_t Stages, uint32_t Paths>
-__global__ void __launch_bounds__(kThreads)
+// The plain uint16 instance (8 KiB stages) is held to four resident CTAs per SM, the others to
+// three (their calibration paths need more registers).
+__global__ void __launch_bounds__(kThreads, (MaxPayload == 8192 && !(Paths & kCal)) ? 4 : 3)
     decode_kernel(const tsk_decode_task *__restrict__ tasks, uint32_t ntasks,
                   const tsk_decode_image *__restrict__ images,
                   const tsk_row_start *__restrict__ rowtab, tsk_result *results) {
@@ -549,34 +596,25 @@ __global__ void __launch_bounds__(kThreads)
         }
         if (ok) {
             Ctx x;
-            const uint64_t esize = calibrated || f32 ? 4u : 2u;
-            const uint64_t pitch = im->out_pitch;
-            x.pitch = pitch;
-            x.out = reinterpret_cast<uint8_t *>(im->out) + t.oy * pitch +
-                    (static_cast<int64_t>(t.ox) - t.col0) * static_cast<int64_t>(esize);
+            x.out = reinterpret_cast<uint8_t *>(t.dst);
+            x.pitch = t.pitch;
             x.w = t.width;
             x.row0 = t.row0;
             x.row1 = t.row1;
             x.col0 = t.col0;
             x.col1 = t.col1;
+            x.full = (t.flags & TSK_FULL) != 0;
             x.omap = x.gmap = nullptr;
             x.opitch = x.gpitch = 0;
             x.offset = 0.0f;
             x.gain = 1.0f;
             if (calibrated) {
-                const int64_t cx = static_cast<int64_t>(t.ox) - t.col0;
-                x.offset = im->offset;
-                x.gain = im->gain;
-                x.opitch = im->offset_pitch;
-                x.gpitch = im->gain_pitch;
-                if (im->offset_map) {
-                    x.omap = reinterpret_cast<const uint8_t *>(im->offset_map) + t.oy * x.opitch +
-                             cx * 4;
-                }
-                if (im->gain_map) {
-                    x.gmap = reinterpret_cast<const uint8_t *>(im->gain_map) + t.oy * x.gpitch +
-                             cx * 4;
-                }
+                x.offset = h.offset;
+                x.gain = h.gain;
+                x.opitch = h.opitch;
+                x.gpitch = h.gpitch;
+                x.omap = reinterpret_cast<const uint8_t *>(h.omap);
+                x.gmap = reinterpret_cast<const uint8_t *>(h.gmap);
             }
             const uint16_t *rows = sh.rows[s];
             if constexpr ((Paths & kU16) && (Paths & kPlain)) {

@@ -25,6 +25,7 @@ enum {
     TSK_CALIBRATED = 2, // output is calibrated FP32
     TSK_TRUSTED = 4,    // index entry and rows are read on the device (encoder output)
     TSK_FIRST = 8,      // first task of its image: writes the image's result record
+    TSK_FULL = 16,      // every column of full-width rows is written, to 16-byte-aligned rows
 };
 
 // Largest payload of one tile: RAW FP32, 4096 samples.
@@ -32,16 +33,20 @@ enum {
 #define TSK_MAX_ROWS 64
 #define TSK_PAYLOAD_BYTES 16384
 
-// One tile to decode. 48 bytes.
+// One tile to decode. 64 bytes, self-contained: a consumer needs nothing else but the payload.
 typedef struct __align__(16) {
     // Parsed: device address of the tile payload. Trusted: device address of the archive.
     uint64_t src;
     // Parsed: payload length in 32-bit words. Trusted: the tile's index in the archive.
     uint64_t words_or_tile;
+    // Output address of tile column 0 in tile row row0 (may lie before the region when the ROI
+    // starts inside the tile; only columns [col0, col1) are written), and the output pitch.
+    uint64_t dst;
+    uint64_t pitch;
     uint32_t image;   // slot in the image table and the result buffer
     uint32_t rows_at; // parsed PREDICT: first entry of this tile's row table
-    uint32_t ox;      // output column of tile column col0
-    uint32_t oy;      // output row of tile row row0
+    uint32_t ox;      // output column of tile column col0 (calibration maps)
+    uint32_t oy;      // output row of tile row row0 (calibration maps)
     uint16_t width;   // actual tile width
     uint16_t height;  // actual tile height
     uint16_t row0, row1; // tile rows written: [row0, row1)
