@@ -102,8 +102,48 @@ struct Ctx {
     uint64_t gpitch;
     float offset, gain;
     uint32_t w, row0, row1, col0, col1;
-    bool full; // TSK_FULL: whole rows of a class width, 16-byte-aligned rows
+    bool full;         // TSK_FULL: whole rows of a class width, 16-byte-aligned rows
+    uint32_t one, top; // runtime constants 1 and 0x80000000 (see Pipes)
 };
+
+// Pipe balance. On this SM the integer ALU pipe (logic, shifts, adds) and the FMA pipe
+// (integer multiply-add) each run at half the issue rate, and the uint16 decode is ALU-bound.
+// Additions written as multiply-adds by a runtime 1 (a kernel argument the compiler cannot
+// fold) execute on the FMA pipe instead; so does the left shift by 31 of the sign extraction.
+struct Pipes {
+    uint32_t one; // 1
+    uint32_t top; // 0x80000000
+};
+
+__device__ __forceinline__ uint32_t fma_add(uint32_t a, uint32_t b, const Pipes &p) {
+    uint32_t d;
+    asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(p.one), "r"(b));
+    return d;
+}
+
+// All ones when bit 0 of z is set, else zero: (z << 31) >> 31 (arithmetic), the shift as an
+// FMA-pipe multiply.
+__device__ __forceinline__ uint32_t low_bit_mask(uint32_t z, const Pipes &p) {
+    uint32_t d;
+    asm("mul.lo.u32 %0, %1, %2;" : "=r"(d) : "r"(z), "r"(p.top));
+    return static_cast<uint32_t>(static_cast<int32_t>(d) >> 31);
+}
+
+// uint16 rows (b <= 16): the 64-bit window of the packed words that starts at the bit of item
+// `first` (item c holds residual c - 1). Item 0 starts b bits before the packed words, inside
+// the row descriptor's width word, whose top 16 bits are zero in every accepted file (the
+// reserved bytes are zero and b <= 16): item 0 therefore reads as zero, and the seed enters as
+// the scan's initial carry.
+__device__ __forceinline__ void window16(const uint32_t *packed, uint32_t first, uint32_t b,
+                                         uint32_t &x0, uint32_t &x1) {
+    const int32_t pos = static_cast<int32_t>(first * b) - static_cast<int32_t>(b);
+    const int32_t q = pos >> 5; // -1 for item 0
+    const uint32_t s = static_cast<uint32_t>(pos) & 31u;
+    const uint32_t *w = packed + q;
+    const uint32_t w0 = w[0], w1 = w[1], w2 = w[2];
+    x0 = __funnelshift_r(w0, w1, s);
+    x1 = __funnelshift_r(w1, w2, s);
+}
 
 // Keeps only the first nbits bits of the 64-bit window (x1:x0); used for the lanes whose group
 // runs past the end of a partial row.
@@ -137,15 +177,21 @@ __device__ __forceinline__ void window(const uint32_t *packed, uint32_t first, u
 // Partial: the group may run past the end of the row (those items become zero).
 template <uint32_t G, bool F32, bool Partial>
 __device__ __forceinline__ void terms(const uint32_t *packed, uint32_t c0, uint32_t w, uint32_t b,
-                                      uint32_t (&t)[G]) {
+                                      const Pipes &pipes, uint32_t (&t)[G]) {
     if constexpr (!F32) {
         // uint16, b <= 16: four residuals per 64-bit window.
-        const uint32_t mh = low_mask(b) >> 1;   // the magnitude bits of a zigzag value
-        const uint32_t sign = b != 0 ? 1u : 0u; // its sign bit (none when b = 0)
+        if (b == 0) {
+#pragma unroll
+            for (uint32_t k = 0; k < G; ++k) {
+                t[k] = 0;
+            }
+            return;
+        }
+        const uint32_t mh = low_mask(b) >> 1; // the magnitude bits of a zigzag value
 #pragma unroll
         for (uint32_t q = 0; q < G; q += 4) {
             uint32_t x0, x1;
-            window(packed, c0 + q, b, x0, x1);
+            window16(packed, c0 + q, b, x0, x1);
             if constexpr (Partial) {
                 if (c0 + q + 4 > w) {
                     const uint32_t items = w > c0 + q ? w - (c0 + q) : 0u;
@@ -162,7 +208,7 @@ __device__ __forceinline__ void terms(const uint32_t *packed, uint32_t c0, uint3
 #pragma unroll
             for (uint32_t k = 0; k < 4; ++k) {
                 // Inverse zigzag as an unsigned delta: z/2 or -(z/2) - 1, modulo 2^32.
-                t[q + k] = ((z[k] >> 1) & mh) ^ (0u - (z[k] & sign));
+                t[q + k] = ((z[k] >> 1) & mh) ^ low_bit_mask(z[k], pipes);
             }
         }
     } else {
@@ -298,6 +344,15 @@ __device__ void decode_rows(const Ctx &x, const uint32_t *payload, const uint16_
     const uint32_t sub = lane % LW;
     const uint32_t w = x.w;
     const uint32_t passes = (x.col1 + kSpan - 1) / kSpan;
+    const Pipes pipes{x.one, x.top};
+    // The scan's combine: XOR for FP32 words, addition (on the FMA pipe) for uint16.
+    auto add = [&pipes](uint32_t a, uint32_t b) {
+        if constexpr (F32) {
+            return a ^ b;
+        } else {
+            return fma_add(a, b, pipes);
+        }
+    };
     for (uint32_t base = x.row0 + warp * kRowsPerWarp; base < x.row1;
          base += kConsumerWarps * kRowsPerWarp) {
         const uint32_t r = base + lane / LW;
@@ -319,7 +374,7 @@ __device__ void decode_rows(const Ctx &x, const uint32_t *payload, const uint16_
                 const uint32_t c0 = pass * kSpan + sub * G;
                 uint32_t t[G];
                 if (Full || c0 < w) {
-                    terms<G, F32, !Full>(packed, c0, w, b, t);
+                    terms<G, F32, !Full>(packed, c0, w, b, pipes, t);
                 } else {
 #pragma unroll
                     for (uint32_t k = 0; k < G; ++k) {
@@ -328,7 +383,7 @@ __device__ void decode_rows(const Ctx &x, const uint32_t *payload, const uint16_
                 }
 #pragma unroll
                 for (uint32_t k = 1; k < G; ++k) {
-                    t[k] = combine<F32>(t[k - 1], t[k]);
+                    t[k] = add(t[k - 1], t[k]);
                 }
                 const uint32_t total = t[G - 1];
                 uint32_t inclusive = total;
@@ -336,16 +391,16 @@ __device__ void decode_rows(const Ctx &x, const uint32_t *payload, const uint16_
                 for (uint32_t d = 1; d < LW; d <<= 1) {
                     const uint32_t other = __shfl_up_sync(kFull, inclusive, d, LW);
                     if (sub >= d) {
-                        inclusive = combine<F32>(other, inclusive);
+                        inclusive = add(other, inclusive);
                     }
                 }
-                const uint32_t before = combine<F32>(carry, uncombine<F32>(inclusive, total));
-                carry = combine<F32>(carry, __shfl_sync(kFull, inclusive, LW - 1, LW));
+                const uint32_t before = add(carry, uncombine<F32>(inclusive, total));
+                carry = add(carry, __shfl_sync(kFull, inclusive, LW - 1, LW));
                 if (live) {
                     uint32_t v[G];
 #pragma unroll
                     for (uint32_t k = 0; k < G; ++k) {
-                        v[k] = combine<F32>(before, t[k]);
+                        v[k] = add(before, t[k]);
                     }
                     store<G, F32, Cal, Full>(x, line, orow, grow, c0, v);
                 }
@@ -530,7 +585,8 @@ template <uint32_t MaxPayload, uint32_t Stages, uint32_t Paths>
 __global__ void __launch_bounds__(kThreads, (MaxPayload == 8192 && !(Paths & kCal)) ? 4 : 3)
     decode_kernel(const tsk_decode_task *__restrict__ tasks, uint32_t ntasks,
                   const tsk_decode_image *__restrict__ images,
-                  const tsk_row_start *__restrict__ rowtab, tsk_result *results) {
+                  const tsk_row_start *__restrict__ rowtab, tsk_result *results, uint32_t one,
+                  uint32_t top) {
     using Sh = Shared<MaxPayload, Stages>;
     extern __shared__ __align__(128) uint8_t smem_raw[];
     Sh &sh = *reinterpret_cast<Sh *>(smem_raw);
@@ -604,6 +660,8 @@ __global__ void __launch_bounds__(kThreads, (MaxPayload == 8192 && !(Paths & kCa
             x.col0 = t.col0;
             x.col1 = t.col1;
             x.full = (t.flags & TSK_FULL) != 0;
+            x.one = one;
+            x.top = top;
             x.omap = x.gmap = nullptr;
             x.opitch = x.gpitch = 0;
             x.offset = 0.0f;
@@ -665,7 +723,7 @@ __global__ void __launch_bounds__(kThreads, (MaxPayload == 8192 && !(Paths & kCa
 }
 
 using KernelFn = void (*)(const tsk_decode_task *, uint32_t, const tsk_decode_image *,
-                          const tsk_row_start *, tsk_result *);
+                          const tsk_row_start *, tsk_result *, uint32_t, uint32_t);
 
 struct Variant {
     KernelFn fn;
@@ -725,6 +783,7 @@ extern "C" int tsk_decode_launch(const tsk_decode_task *tasks, uint32_t ntasks,
                                  cudaStream_t stream) {
     if (ntasks == 0) return cudaSuccess;
     const tsk::Variant v = tsk::select(config.paths);
-    v.fn<<<config.grid, tsk::kThreads, v.smem, stream>>>(tasks, ntasks, images, rows, results);
+    v.fn<<<config.grid, tsk::kThreads, v.smem, stream>>>(tasks, ntasks, images, rows, results, 1u,
+                                                         0x80000000u);
     return cudaGetLastError();
 }
