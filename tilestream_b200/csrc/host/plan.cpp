@@ -628,6 +628,19 @@ bool upload(void *storage, std::uint64_t at, const std::vector<T> &v, cudaStream
                                         stream) == cudaSuccess;
 }
 
+// Kernel shape of the plain uint16 decoder (consumer warps x columns per lane, see
+// tsk_decode_config.shape). The default, 4 consumer warps with 16 columns per lane, measured
+// fastest of the four on B200 for all three tile geometries; TILESTREAM_DECODE_SHAPE overrides
+// it for tuning runs.
+std::uint32_t decode_shape() {
+    static const std::uint32_t shape = [] {
+        const char *env = std::getenv("TILESTREAM_DECODE_SHAPE");
+        return env != nullptr ? static_cast<std::uint32_t>(std::strtoul(env, nullptr, 10)) % 4
+                              : 2u;
+    }();
+    return shape;
+}
+
 Status build(const BatchRequest &request, PlanState &plan, cudaStream_t stream) {
     plan.operation = request.operation;
     plan.count = request.count;
@@ -718,6 +731,7 @@ Status build(const BatchRequest &request, PlanState &plan, cudaStream_t stream) 
             (d.type == PixelType::float32 ? TSK_PATH_F32 : TSK_PATH_U16) |
             (request.operation == Operation::decode_calibrate ? TSK_PATH_CALIBRATED
                                                               : TSK_PATH_PLAIN);
+        plan.config.shape = decode_shape();
         err = tsk_decode_prepare(&plan.config, plan.task_count, plan.device);
         break;
     }

@@ -35,10 +35,12 @@
 namespace tsk {
 namespace {
 
-constexpr uint32_t kConsumerWarps = 8;
-constexpr uint32_t kConsumers = kConsumerWarps * 32;
-constexpr uint32_t kThreads = kConsumers + 32;
 constexpr uint32_t kFull = 0xffffffffu;
+
+// Threads of a CTA with CW consumer warps and the producer warp.
+constexpr uint32_t threads_of(uint32_t cw) {
+    return cw * 32 + 32;
+}
 
 enum : uint32_t { kStageOk = 0, kStageSkip = 1, kStageMalformed = 2 };
 
@@ -309,14 +311,19 @@ __device__ __forceinline__ void store(const Ctx &x, uint8_t *line, const uint8_t
         }
     } else {
         uint16_t *dst = reinterpret_cast<uint16_t *>(line) + c0;
-        if (Full || (whole && (reinterpret_cast<uintptr_t>(dst) & (2 * G - 1)) == 0)) {
+        constexpr uintptr_t kAlign = G >= 8 ? 15u : 2 * G - 1;
+        if (Full || (whole && (reinterpret_cast<uintptr_t>(dst) & kAlign) == 0)) {
             uint32_t p[G / 2];
 #pragma unroll
             for (uint32_t k = 0; k < G / 2; ++k) {
                 p[k] = __byte_perm(v[2 * k], v[2 * k + 1], 0x5410);
             }
-            if constexpr (G == 8) {
-                *reinterpret_cast<uint4 *>(dst) = make_uint4(p[0], p[1], p[2], p[3]);
+            if constexpr (G >= 8) {
+#pragma unroll
+                for (uint32_t k = 0; k < G / 2; k += 4) {
+                    *reinterpret_cast<uint4 *>(dst + 2 * k) =
+                        make_uint4(p[k], p[k + 1], p[k + 2], p[k + 3]);
+                }
             } else {
                 *reinterpret_cast<uint2 *>(dst) = make_uint2(p[0], p[1]);
             }
@@ -332,10 +339,10 @@ __device__ __forceinline__ void store(const Ctx &x, uint8_t *line, const uint8_t
     }
 }
 
-// Decodes rows [row0, row1) of one staged tile with the 8 consumer warps; LW lanes per row.
+// Decodes rows [row0, row1) of one staged tile with the CW consumer warps; LW lanes per row.
 // Full: the tile's width is G * LW (or twice that for FP32 256-wide rows) and every column is
 // written to aligned rows, so no per-group bounds or alignment checks are needed.
-template <uint32_t G, uint32_t LW, bool F32, bool Cal, bool Full>
+template <uint32_t CW, uint32_t G, uint32_t LW, bool F32, bool Cal, bool Full>
 __device__ void decode_rows(const Ctx &x, const uint32_t *payload, const uint16_t *rows,
                             uint32_t mode) {
     constexpr uint32_t kRowsPerWarp = 32 / LW;
@@ -354,7 +361,7 @@ __device__ void decode_rows(const Ctx &x, const uint32_t *payload, const uint16_
         }
     };
     for (uint32_t base = x.row0 + warp * kRowsPerWarp; base < x.row1;
-         base += kConsumerWarps * kRowsPerWarp) {
+         base += CW * kRowsPerWarp) {
         const uint32_t r = base + lane / LW;
         const bool live = r < x.row1;
         const uint64_t line_off = static_cast<uint64_t>(live ? r - x.row0 : 0u);
@@ -429,33 +436,34 @@ __device__ void decode_rows(const Ctx &x, const uint32_t *payload, const uint16_
     }
 }
 
-template <uint32_t G, uint32_t LW, bool F32, bool Cal>
+template <uint32_t CW, uint32_t G, uint32_t LW, bool F32, bool Cal>
 __device__ __forceinline__ void decode_class(const Ctx &x, const uint32_t *payload,
                                              const uint16_t *rows, uint32_t mode) {
     if (x.full) {
-        decode_rows<G, LW, F32, Cal, true>(x, payload, rows, mode);
+        decode_rows<CW, G, LW, F32, Cal, true>(x, payload, rows, mode);
     } else {
-        decode_rows<G, LW, F32, Cal, false>(x, payload, rows, mode);
+        decode_rows<CW, G, LW, F32, Cal, false>(x, payload, rows, mode);
     }
 }
 
-// Width classes: uint16 rows take 8 columns per lane, FP32 rows 4.
-template <bool F32, bool Cal>
+// Width classes: a row of the class width is covered by LW = width / G lanes. uint16 rows take
+// G16 columns per lane (8 or 16), FP32 rows 4.
+template <uint32_t CW, uint32_t G16, bool F32, bool Cal>
 __device__ __forceinline__ void decode_tile(const Ctx &x, const uint32_t *payload,
                                             const uint16_t *rows, uint32_t mode) {
     if constexpr (!F32) {
         if (x.w > 128) {
-            decode_class<8, 32, false, Cal>(x, payload, rows, mode);
+            decode_class<CW, G16, 256 / G16, false, Cal>(x, payload, rows, mode);
         } else if (x.w > 64) {
-            decode_class<8, 16, false, Cal>(x, payload, rows, mode);
+            decode_class<CW, G16, 128 / G16, false, Cal>(x, payload, rows, mode);
         } else {
-            decode_class<8, 8, false, Cal>(x, payload, rows, mode);
+            decode_class<CW, G16, 64 / G16, false, Cal>(x, payload, rows, mode);
         }
     } else {
         if (x.w > 64) {
-            decode_class<4, 32, true, Cal>(x, payload, rows, mode);
+            decode_class<CW, 4, 32, true, Cal>(x, payload, rows, mode);
         } else {
-            decode_class<4, 16, true, Cal>(x, payload, rows, mode);
+            decode_class<CW, 4, 16, true, Cal>(x, payload, rows, mode);
         }
     }
 }
@@ -579,29 +587,30 @@ __device__ void stage_task(Sh &sh, uint32_t s, const tsk_decode_task &t,
     mbar_arrive(&sh.full[s]);
 }
 
-template <uint32_t MaxPayload, uint32_t Stages, uint32_t Paths>
-// The plain uint16 instance (8 KiB stages) is held to four resident CTAs per SM, the others to
-// three (their calibration paths need more registers).
-__global__ void __launch_bounds__(kThreads, (MaxPayload == 8192 && !(Paths & kCal)) ? 4 : 3)
+// CW consumer warps, G16 columns per lane for uint16 rows; MinBlocks resident CTAs per SM.
+template <uint32_t MaxPayload, uint32_t Stages, uint32_t Paths, uint32_t CW, uint32_t G16,
+          uint32_t MinBlocks>
+__global__ void __launch_bounds__(threads_of(CW), MinBlocks)
     decode_kernel(const tsk_decode_task *__restrict__ tasks, uint32_t ntasks,
                   const tsk_decode_image *__restrict__ images,
                   const tsk_row_start *__restrict__ rowtab, tsk_result *results, uint32_t one,
                   uint32_t top) {
     using Sh = Shared<MaxPayload, Stages>;
+    constexpr uint32_t kConsumers = CW * 32;
     extern __shared__ __align__(128) uint8_t smem_raw[];
     Sh &sh = *reinterpret_cast<Sh *>(smem_raw);
     const uint32_t warp = threadIdx.x / 32, lane = threadIdx.x % 32;
     if (threadIdx.x == 0) {
         for (uint32_t s = 0; s < Stages; ++s) {
             mbar_init(&sh.full[s], 1);
-            mbar_init(&sh.empty[s], kConsumerWarps);
+            mbar_init(&sh.empty[s], CW);
         }
         fence_barrier_init();
     }
     __syncthreads();
     const uint32_t mine = blockIdx.x < ntasks ? (ntasks - 1 - blockIdx.x) / gridDim.x + 1 : 0;
 
-    if (warp == kConsumerWarps) {
+    if (warp == CW) {
         // Producer warp: lane 0 issues everything. The next task record is loaded before
         // waiting for a free stage, so its latency overlaps the consumers' work.
         if (lane != 0) {
@@ -676,16 +685,18 @@ __global__ void __launch_bounds__(kThreads, (MaxPayload == 8192 && !(Paths & kCa
             }
             const uint16_t *rows = sh.rows[s];
             if constexpr ((Paths & kU16) && (Paths & kPlain)) {
-                if (!f32 && !calibrated) decode_tile<false, false>(x, payload, rows, hmode);
+                if (!f32 && !calibrated) {
+                    decode_tile<CW, G16, false, false>(x, payload, rows, hmode);
+                }
             }
             if constexpr ((Paths & kF32) && (Paths & kPlain)) {
-                if (f32 && !calibrated) decode_tile<true, false>(x, payload, rows, hmode);
+                if (f32 && !calibrated) decode_tile<CW, G16, true, false>(x, payload, rows, hmode);
             }
             if constexpr ((Paths & kU16) && (Paths & kCal)) {
-                if (!f32 && calibrated) decode_tile<false, true>(x, payload, rows, hmode);
+                if (!f32 && calibrated) decode_tile<CW, G16, false, true>(x, payload, rows, hmode);
             }
             if constexpr ((Paths & kF32) && (Paths & kCal)) {
-                if (f32 && calibrated) decode_tile<true, true>(x, payload, rows, hmode);
+                if (f32 && calibrated) decode_tile<CW, G16, true, true>(x, payload, rows, hmode);
             }
         }
         __syncwarp();
@@ -728,19 +739,35 @@ using KernelFn = void (*)(const tsk_decode_task *, uint32_t, const tsk_decode_im
 struct Variant {
     KernelFn fn;
     size_t smem;
+    uint32_t threads;
 };
 
 // Kernel instances: uint16-only plans stage 8 KiB tiles (four stages), plans with FP32 stage
 // 16 KiB tiles (three stages); the calibrated and plain paths are separate instances so that a
-// plan's kernel carries only the code (and registers) it needs.
-template <uint32_t MaxPayload, uint32_t Stages, uint32_t Paths> Variant make() {
-    return {decode_kernel<MaxPayload, Stages, Paths>, sizeof(Shared<MaxPayload, Stages>)};
+// plan's kernel carries only the code (and registers) it needs. The plain uint16 path, the
+// headline one, comes in four shapes (consumer warps x columns per lane) for the tuner.
+template <uint32_t MaxPayload, uint32_t Stages, uint32_t Paths, uint32_t CW = 8,
+          uint32_t G16 = 8, uint32_t MinBlocks = 3>
+Variant make() {
+    return {decode_kernel<MaxPayload, Stages, Paths, CW, G16, MinBlocks>,
+            sizeof(Shared<MaxPayload, Stages>), threads_of(CW)};
 }
 
-Variant select(uint32_t paths) {
+Variant select(uint32_t paths, uint32_t shape) {
     const bool f32 = paths & kF32, u16 = paths & kU16, plain = paths & kPlain, c = paths & kCal;
     if (!f32) {
-        if (plain && !c) return make<8192, 4, kU16 | kPlain>();
+        if (plain && !c) {
+            switch (shape) {
+            case 1:
+                return make<8192, 4, kU16 | kPlain, 8, 16, 3>();
+            case 2:
+                return make<8192, 4, kU16 | kPlain, 4, 16, 5>();
+            case 3:
+                return make<8192, 4, kU16 | kPlain, 4, 8, 6>();
+            default:
+                return make<8192, 4, kU16 | kPlain, 8, 8, 4>();
+            }
+        }
         if (c && !plain) return make<8192, 4, kU16 | kCal>();
         return make<8192, 4, kU16 | kPlain | kCal>();
     }
@@ -755,14 +782,14 @@ Variant select(uint32_t paths) {
 } // namespace tsk
 
 // Sets the kernel instance's shared-memory limit (which also loads it) and fills in the
-// occupancy-derived persistent grid for the plan's path mask.
+// occupancy-derived persistent grid for the plan's path mask and kernel shape.
 extern "C" int tsk_decode_prepare(tsk_decode_config *config, uint32_t ntasks, int device) {
-    const tsk::Variant v = tsk::select(config->paths);
+    const tsk::Variant v = tsk::select(config->paths, config->shape);
     cudaError_t e = cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(v.smem));
     if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v.fn, tsk::kThreads, v.smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v.fn, v.threads, v.smem);
     if (e != cudaSuccess) return e;
     int sms = 0;
     e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
@@ -782,8 +809,8 @@ extern "C" int tsk_decode_launch(const tsk_decode_task *tasks, uint32_t ntasks,
                                  tsk_result *results, tsk_decode_config config,
                                  cudaStream_t stream) {
     if (ntasks == 0) return cudaSuccess;
-    const tsk::Variant v = tsk::select(config.paths);
-    v.fn<<<config.grid, tsk::kThreads, v.smem, stream>>>(tasks, ntasks, images, rows, results, 1u,
-                                                         0x80000000u);
+    const tsk::Variant v = tsk::select(config.paths, config.shape);
+    v.fn<<<config.grid, v.threads, v.smem, stream>>>(tasks, ntasks, images, rows, results, 1u,
+                                                     0x80000000u);
     return cudaGetLastError();
 }

@@ -96,6 +96,7 @@ typedef struct {
     uint32_t per_sm; // resident CTAs per SM at the kernel's occupancy
     uint32_t smem;   // dynamic shared memory per CTA in bytes
     uint32_t paths;  // TSK_PATH_* mask selecting the kernel instance
+    uint32_t shape;  // plain uint16 kernel shape (consumer warps x columns per lane), 0-3
 } tsk_decode_config;
 
 // One image to encode. 96 bytes.
