@@ -126,6 +126,27 @@ int ts_calibrate_async(const ts_plan *plan, ts_mutable_bytes workspace, ts_resul
 int ts_decode_calibrate_async(const ts_plan *plan, ts_mutable_bytes workspace,
                               ts_result_buffer results, void *stream);
 
+/* ---- allocation-free encode (no counterpart in the reference) ------------------------------
+ * Encodes one image into a complete .tsc file on the GPU, like a one-item compress plan, but
+ * allocates no memory: no plan tables, no workspace, no cudaMalloc or cudaFree. It is for
+ * callers that cannot allocate device memory while they encode - a process whose GPU memory is
+ * fully reserved by another allocator, an acquisition loop that must not stall on an allocator
+ * or an implicit device synchronization, a deployment that forbids dynamic allocation after
+ * initialization. Its scratch is a fixed 1 MiB array in device memory that the library holds
+ * on every GPU it is loaded on, which limits one image to ts_compress_noalloc_max_tiles()
+ * tiles (131,070: for example 16384 x 32768 pixels with 128x32 tiles); larger images return
+ * resource_limit and nothing is written.
+ *
+ * input, output and result are device memory of the current device; output needs
+ * compress_bound bytes and result one ts_device_result. Arguments are checked as for
+ * compress_async, statuses are the same, and per-image completion is written to *result.
+ * The first call on each device sets up that device's scratch address and must therefore
+ * come before any stream capture on it. Every call shares the array and clears what it uses:
+ * calls that overlap on one GPU race, so order them on one stream or with events. */
+int ts_compress_noalloc(ts_const_image_view input, ts_tile_shape tile, ts_mutable_bytes output,
+                        ts_device_result *result, void *stream);
+uint64_t ts_compress_noalloc_max_tiles(void);
+
 /* ---- device buffers and completion (cuda.h:113-145) ----------------------------------------
  * Stream-ordered allocation aligned to 256 bytes; *data is replaced only on success. */
 int ts_device_allocate(uint64_t bytes, void *stream, void **data);

@@ -131,6 +131,8 @@ _SIGNATURES = {
     "ts_decode_roi_async": (C.c_int, [vp, MutableBytes, ResultBuffer, vp]),
     "ts_calibrate_async": (C.c_int, [vp, MutableBytes, ResultBuffer, vp]),
     "ts_decode_calibrate_async": (C.c_int, [vp, MutableBytes, ResultBuffer, vp]),
+    "ts_compress_noalloc": (C.c_int, [ConstImageView, TileShape, MutableBytes, vp, vp]),
+    "ts_compress_noalloc_max_tiles": (u64, []),
     "ts_device_allocate": (C.c_int, [u64, vp, C.POINTER(vp)]),
     "ts_device_release": (C.c_int, [vp, vp]),
     "ts_synchronize": (C.c_int, [vp]),

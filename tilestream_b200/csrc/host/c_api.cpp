@@ -279,3 +279,83 @@ int ts_info_json(char *buf, uint64_t capacity, uint64_t *needed) {
 }
 
 } // extern "C"
+
+// Allocation-free one-image encode (declared in include/tilestream_c.h; no counterpart in the
+// reference). Host checks follow compress_async's (draft_compress and check_execution in
+// plan.cpp), then the image is encoded with the static scratch of encode.cu.
+extern "C" uint64_t ts_compress_noalloc_max_tiles(void) {
+    return tsk_encode_static_max_tiles();
+}
+
+extern "C" int ts_compress_noalloc(ts_const_image_view input_c, ts_tile_shape tile_c,
+                                   ts_mutable_bytes output_c, ts_device_result *result,
+                                   void *stream_v) {
+    namespace d = ts::cuda::detail;
+    const auto input = as<ts::ConstImageView>(input_c);
+    const auto tile = as<ts::TileShape>(tile_c);
+    const auto output = as<ts::MutableBytes>(output_c);
+    const cudaStream_t stream = stream_of(stream_v);
+    ts::Status st = ts::host::view_ok(input);
+    if (st != ts::Status::success) {
+        return code(st);
+    }
+    std::uint64_t bound = 0;
+    st = ts::compress_bound(input.image, tile, bound);
+    if (st != ts::Status::success) {
+        return code(st);
+    }
+    st = ts::host::byte_range(output.data, output.size);
+    if (st != ts::Status::success) {
+        return code(st);
+    }
+    if (output.data == nullptr || reinterpret_cast<std::uintptr_t>(output.data) % 4 != 0) {
+        return code(ts::Status::invalid_argument);
+    }
+    if (output.size < bound) {
+        return code(ts::Status::buffer_too_small);
+    }
+    if (result == nullptr || reinterpret_cast<std::uintptr_t>(result) % alignof(ts::DeviceResult)) {
+        return code(ts::Status::invalid_argument);
+    }
+    if (ts::host::overlaps(input.data, input.capacity_bytes, output.data, output.size) ||
+        ts::host::overlaps(result, sizeof(ts::DeviceResult), output.data, output.size) ||
+        ts::host::overlaps(result, sizeof(ts::DeviceResult), input.data, input.capacity_bytes)) {
+        return code(ts::Status::invalid_argument);
+    }
+    tsk_encode_image image{};
+    image.columns = ts::host::ceil_div(input.image.width, tile.width);
+    image.tile_count = image.columns * ts::host::ceil_div(input.image.height, tile.height);
+    if (image.tile_count > tsk_encode_static_max_tiles()) {
+        return code(ts::Status::resource_limit);
+    }
+    int device = 0, pageable = 0;
+    if (cudaGetDevice(&device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&pageable, cudaDevAttrPageableMemoryAccess, device) != cudaSuccess) {
+        return code(d::cuda_failure("cudaGetDevice/cudaDeviceGetAttribute"));
+    }
+    st = d::stream_device(stream, device);
+    for (const void *p : {input.data, static_cast<const void *>(output.data),
+                          static_cast<const void *>(result)}) {
+        if (st == ts::Status::success) {
+            st = d::accessible(p, device, pageable != 0);
+        }
+    }
+    if (st == ts::Status::success && cudaPeekAtLastError() != cudaSuccess) {
+        st = ts::Status::cuda_error; // the caller's pending error is left for the caller
+    }
+    if (st != ts::Status::success) {
+        return code(st);
+    }
+    image.input = reinterpret_cast<std::uint64_t>(input.data);
+    image.pitch = input.pitch_bytes;
+    image.output = reinterpret_cast<std::uint64_t>(output.data);
+    image.first_tile = 0;
+    image.width = input.image.width;
+    image.height = input.image.height;
+    image.tile_width = tile.width;
+    image.tile_height = tile.height;
+    image.type = static_cast<std::uint32_t>(input.image.type);
+    return code(d::cuda_status(
+        tsk_encode_static_launch(&image, reinterpret_cast<tsk_result *>(result), stream),
+        "allocation-free encode launch"));
+}

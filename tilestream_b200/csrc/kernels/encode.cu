@@ -22,6 +22,7 @@
 #include "tasks.h"
 
 #include <cstdint>
+#include <mutex>
 
 namespace tsk {
 namespace {
@@ -401,5 +402,123 @@ extern "C" int tsk_encode_launch(const tsk_encode_image *images, uint32_t image_
     if (grid > total_tiles) grid = total_tiles;
     tsk::encode_kernel<<<static_cast<uint32_t>(grid), tsk::kThreads, smem, stream>>>(
         images, image_count, total_tiles, static_cast<uint64_t *>(state), results);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------------------------
+// Allocation-free encoding of one image.
+//
+// Some callers cannot allocate device memory when they encode: a process whose GPU memory is
+// already reserved in full by another allocator (a framework's caching pool, say), an acquisition
+// loop that must not risk an allocator stall or an implicit device synchronization per frame,
+// or a deployment that forbids dynamic allocation after initialization. The plan-based
+// compress_async path needs device tables from prepare_batch and a caller-allocated workspace;
+// this variant needs neither. Its only scratch, the tile counter and look-back flags, lives in
+// the file-scope array below, which every GPU that loads the library holds until the process
+// exits.
+//
+// Every call shares that array, and each call clears the part it uses before its kernel runs.
+// Two calls that overlap on the same GPU (different streams without an ordering dependency)
+// therefore race and corrupt each other's output: order them on one stream or with events.
+namespace tsk {
+namespace {
+
+// At most this many tiles per image: 8 bytes of state per tile plus two words, 1 MiB in all.
+constexpr uint64_t kStaticStateWords = 131072;
+
+__device__ __align__(256) uint64_t g_encode_scratch[kStaticStateWords];
+
+__global__ void __launch_bounds__(kThreads)
+    encode_kernel_static(tsk_encode_image image, uint64_t total_tiles, uint64_t *state,
+                         tsk_result *result) {
+    extern __shared__ __align__(16) uint8_t smem_raw[];
+    EncodeShared &sh = *reinterpret_cast<EncodeShared *>(smem_raw);
+    uint64_t *counter = state;
+    uint64_t *flags = state + 2;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const uint64_t id = atomicAdd(reinterpret_cast<unsigned long long *>(counter), 1ull);
+            sh.tile_id = id < total_tiles ? id : total_tiles;
+            sh.image = 0;
+        }
+        __syncthreads();
+        const uint64_t id = sh.tile_id;
+        if (id >= total_tiles) {
+            return;
+        }
+        if (image.type == 2) {
+            encode_tile<true>(sh, image, id, flags, id, result, 0);
+        } else {
+            encode_tile<false>(sh, image, id, flags, id, result, 0);
+        }
+        __syncthreads();
+    }
+}
+
+// Per-device set-up, done by the first call on each device with that device current.
+struct StaticSetup {
+    uint64_t *scratch = nullptr; // device address of g_encode_scratch
+    uint32_t grid = 0;
+};
+
+constexpr int kMaxDevices = 64;
+std::mutex g_setup_mutex;
+StaticSetup g_setup[kMaxDevices];
+
+cudaError_t static_setup(int device, StaticSetup &out) {
+    std::lock_guard<std::mutex> lock(g_setup_mutex);
+    StaticSetup &s = g_setup[device];
+    if (s.scratch == nullptr) {
+        void *address = nullptr;
+        // In host code the name g_encode_scratch is a host-side stand-in, not a device address;
+        // the runtime returns this device's copy of the array.
+        cudaError_t e = cudaGetSymbolAddress(&address, g_encode_scratch);
+        if (e != cudaSuccess) return e;
+        const size_t smem = sizeof(EncodeShared);
+        e = cudaFuncSetAttribute(encode_kernel_static, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(smem));
+        if (e != cudaSuccess) return e;
+        int sms = 0, per_sm = 0;
+        e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        if (e != cudaSuccess) return e;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, encode_kernel_static, kThreads,
+                                                          smem);
+        if (e != cudaSuccess) return e;
+        s.grid = static_cast<uint32_t>(sms * (per_sm > 0 ? per_sm : 1));
+        s.scratch = static_cast<uint64_t *>(address);
+    }
+    out = s;
+    return cudaSuccess;
+}
+
+} // namespace
+} // namespace tsk
+
+extern "C" uint64_t tsk_encode_static_max_tiles(void) {
+    return tsk::kStaticStateWords - 2;
+}
+
+// Encodes one validated image with the static scratch; allocates nothing. Returns a
+// cudaError_t value, or cudaErrorInvalidValue when the image has more tiles than the array holds.
+extern "C" int tsk_encode_static_launch(const tsk_encode_image *image, tsk_result *result,
+                                        cudaStream_t stream) {
+    const uint64_t total = image->tile_count;
+    if (total == 0 || total > tsk_encode_static_max_tiles()) return cudaErrorInvalidValue;
+    int device = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e != cudaSuccess) return e;
+    if (device < 0 || device >= tsk::kMaxDevices) return cudaErrorInvalidDevice;
+    tsk::StaticSetup setup;
+    e = tsk::static_setup(device, setup);
+    if (e != cudaSuccess) return e;
+    // The array keeps the previous call's contents: clear the counter and this call's flags.
+    e = cudaMemsetAsync(setup.scratch, 0, tsk_encode_state_bytes(total), stream);
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(result, 0, sizeof(tsk_result), stream);
+    if (e != cudaSuccess) return e;
+    const uint64_t grid = setup.grid < total ? setup.grid : total;
+    tsk::encode_kernel_static<<<static_cast<uint32_t>(grid), tsk::kThreads,
+                                sizeof(tsk::EncodeShared), stream>>>(*image, total, setup.scratch,
+                                                                     result);
     return cudaGetLastError();
 }

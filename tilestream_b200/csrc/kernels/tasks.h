@@ -161,6 +161,11 @@ int tsk_encode_launch(const tsk_encode_image *images, uint32_t image_count, uint
 int tsk_encode_prepare(int device);
 uint64_t tsk_encode_state_bytes(uint64_t total_tiles);
 
+// One image, scratch in a static device array (no allocation); see encode.cu.
+int tsk_encode_static_launch(const tsk_encode_image *image, tsk_result *result,
+                             cudaStream_t stream);
+uint64_t tsk_encode_static_max_tiles(void);
+
 int tsk_calibrate_launch(const tsk_calib_task *tasks, uint32_t ntasks,
                          const tsk_calib_image *images, uint32_t image_count, tsk_result *results,
                          cudaStream_t stream);
