@@ -426,6 +426,251 @@ def run_reference(args):
     }
 
 
+def encode_on_gpu(torch, stream, inputs, ptype, tile):
+    """Encodes device images of one pixel type with one compress plan (tile geometry `tile`).
+    inputs: list of (flat uint8 device tensor, width, height, pitch). Returns the .tsc files as
+    host bytes (the plan-based GPU encoder, byte-identical to the CPU codec per the tests)."""
+    from tilestream_b200 import api, cuda
+    from tilestream_b200.api import BatchItem, Status, TileShape
+    items, outs = [], []
+    for dev, w, h, pitch in inputs:
+        st, bound = api.compress_bound(api.image_spec(ptype, w, h), TileShape(*tile))
+        out = torch.empty(bound, dtype=torch.uint8, device="cuda")
+        item = BatchItem()
+        item.input = api.const_view(dev, ptype, w, h, pitch, dev.numel())
+        item.compressed_output = api.MutableBytes(out.data_ptr(), bound)
+        items.append(item)
+        outs.append(out)
+    st, plan = cuda.prepare_batch(cuda.make_request(cuda.Operation.compress, items,
+                                                    TileShape(*tile)), None, stream)
+    assert st == Status.success, st
+    ws = torch.empty(max(plan.workspace_bytes(), 256), dtype=torch.uint8, device="cuda")
+    res = torch.zeros(16 * len(items), dtype=torch.uint8, device="cuda")
+    assert cuda.compress_async(plan, ws, res, stream) == Status.success
+    torch.cuda.synchronize()
+    sizes = res.cpu().numpy().view(np.uint64).reshape(-1, 2)[:, 1]
+    return [out[:int(n)].cpu().numpy().tobytes() for out, n in zip(outs, sizes)]
+
+
+def time_graph(torch, stream, fn, steps, warmup):
+    """Captures fn (which enqueues on stream) as a CUDA graph; returns ms per replay."""
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=stream, capture_error_mode="relaxed"):
+        fn()
+    for _ in range(warmup):
+        g.replay()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        g.replay()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def run_calibrated(args, torch, stream, peak):
+    """Config 3: float32 4096x4096 smooth field with special words, fused decode + calibration
+    with per-pixel FP32 offset ~ N(100, 5) and gain ~ U(0.9, 1.1) maps."""
+    from tilestream_b200 import api, cuda, workloads
+    from tilestream_b200.api import BatchItem, CompressedInput, ConstBytes, Status
+    frame = workloads.field_frame(W, H, seed=3)
+    offset, gain = workloads.calibration_maps(W, H, seed=5)
+    dev_frame = torch.from_numpy(frame.view(np.uint8).reshape(-1).copy()).cuda()
+    file = encode_on_gpu(torch, stream, [(dev_frame, W, H, W * 4)], 2, (128, 32))[0]
+    st, meta = api.parse_metadata(file)
+    assert st == Status.success
+    dev_off = torch.from_numpy(offset.view(np.uint8).reshape(-1).copy()).cuda()
+    dev_gain = torch.from_numpy(gain.view(np.uint8).reshape(-1).copy()).cuda()
+    copies = []
+    for _ in range(2):
+        src_dev = torch.from_numpy(np.frombuffer(file, dtype=np.uint8).copy()).cuda()
+        out = torch.empty(W * H * 4, dtype=torch.uint8, device="cuda")
+        plain = torch.empty(W * H * 4, dtype=torch.uint8, device="cuda")
+        src = CompressedInput()
+        src.bytes = ConstBytes(src_dev.data_ptr(), len(file))
+        src.metadata = meta.handle
+        item = BatchItem()
+        item.compressed_input = src
+        item.output = api.view(out, 2, W, H, W * 4)
+        item.roi = api.Roi(0, 0, W, H)
+        item.calibration.offset.kind = cuda.ParameterKind.map
+        item.calibration.offset.map = api.const_view(dev_off, 2, W, H, W * 4)
+        item.calibration.gain.kind = cuda.ParameterKind.map
+        item.calibration.gain.map = api.const_view(dev_gain, 2, W, H, W * 4)
+        st, plan = cuda.prepare_batch(cuda.make_request(cuda.Operation.decode_calibrate, [item]),
+                                      None, stream)
+        assert st == Status.success, st
+        pitem = BatchItem()
+        pitem.compressed_input = src
+        pitem.output = api.view(plain, 2, W, H, W * 4)
+        st, pplan = cuda.prepare_batch(cuda.make_request(cuda.Operation.decompress, [pitem]),
+                                       None, stream)
+        assert st == Status.success, st
+        copies.append({"src": src_dev, "out": out, "plan": plan, "plain": plain, "pplan": pplan})
+    ws = torch.empty(max(copies[0]["plan"].workspace_bytes(), 256), dtype=torch.uint8,
+                     device="cuda")
+    res = torch.zeros(16, dtype=torch.uint8, device="cuda")
+    c = copies[0]
+    assert cuda.decompress_async(c["pplan"], ws, res, stream) == Status.success
+    assert cuda.decode_calibrate_async(c["plan"], ws, res, stream) == Status.success
+    torch.cuda.synchronize()
+    words = c["plain"].cpu().numpy().view(np.uint32)
+    exact = bool(np.array_equal(words, frame.reshape(-1)))
+    got = c["out"].cpu().numpy().view(np.float32)
+    x = frame.reshape(-1).view(np.float32)
+    with np.errstate(all="ignore"):
+        host_form = ((x - offset.reshape(-1)).astype(np.float32) * gain.reshape(-1)).astype(
+            np.float32)
+        ref = (x.astype(np.float64) - offset.reshape(-1).astype(np.float64)) * \
+            gain.reshape(-1).astype(np.float64)
+    same = (got.view(np.uint32) == host_form.view(np.uint32)) | (np.isnan(got) &
+                                                                 np.isnan(host_form))
+    normal = np.isfinite(ref) & (np.abs(ref) >= 2.0 ** -126) & np.isfinite(got)
+    ulp = np.spacing(np.abs(ref[normal]).astype(np.float32)).astype(np.float64)
+    max_ulp = float(np.max(np.abs(got[normal].astype(np.float64) - ref[normal]) / ulp))
+
+    def step(k=[0]):
+        cc = copies[k[0] % 2]
+        k[0] += 1
+        cuda.decode_calibrate_async(cc["plan"], ws, res, stream)
+
+    def both():
+        for cc in copies:
+            cuda.decode_calibrate_async(cc["plan"], ws, res, stream)
+
+    ms = time_graph(torch, stream, both, max(3, args.steps // 100), args.warmup) / 2
+    tiles = meta.tiles
+    alg = int(tiles["length"].sum()) + 32 * len(tiles) + W * H * 4 * 3  # output + 2 maps
+    return {"workload": "float32 4096x4096 field (seed 3), 0.1% special words, fused decode + "
+                        "calibration with FP32 offset and gain maps, tiles 128x32",
+            "launch_us": round(ms * 1e3, 2),
+            "calibrated_gbs": round(W * H * 4 / ms / 1e6, 1),
+            "roofline": {"achieved": round(alg / ms / 1e6, 1), "peak": peak,
+                         "frac": round(alg / ms / 1e6 / peak, 4), "unit": "GB/s",
+                         "algorithmic_bytes_per_launch": alg},
+            "pixels_bit_exact_before_calibration": exact,
+            "calibrated_equals_host_two_rounding_form": bool(np.all(same)),
+            "max_ulp_vs_fp64_normal_results": round(max_ulp, 4),
+            "ulp_bound": 1.5}
+
+
+def run_batched(args, torch, stream, peak):
+    """Config 4: 256 archives with width and height uniform in 257..4096, 70% uint16 / 30%
+    float32, a random tile geometry each, decoded into pitched rows: one mixed batch (one
+    persistent kernel, CUDA graph, autotuned) against per-image plain decode on the same GPU."""
+    from tilestream_b200 import api, cuda, workloads
+    from tilestream_b200.api import BatchItem, CompressedInput, ConstBytes, Status
+    rng = np.random.default_rng(4)
+    n = args.archives
+    dims = rng.integers(257, 4097, size=(n, 2))
+    types = np.where(rng.random(n) < 0.7, 1, 2)
+    shapes = [SHAPES[i] for i in rng.integers(0, 3, n)]
+    frames = []
+    for k in range(n):
+        w, h = int(dims[k, 0]), int(dims[k, 1])
+        if types[k] == 1:
+            f = workloads.detector_frame_torch(w, h, 1000 + k).view(torch.uint8).reshape(-1)
+        else:
+            f = workloads.field_frame_torch(w, h, 1000 + k).view(torch.uint8).reshape(-1)
+        frames.append((f.contiguous(), w, h))
+    files = [None] * n
+    for ptype in (1, 2):
+        for tile in SHAPES:
+            group = [k for k in range(n) if types[k] == ptype and shapes[k] == tile]
+            if group:
+                s = 2 if ptype == 1 else 4
+                encoded = encode_on_gpu(torch, stream, [(frames[k][0], frames[k][1], frames[k][2],
+                                                         frames[k][1] * s) for k in group],
+                                        ptype, tile)
+                for k, f in zip(group, encoded):
+                    files[k] = f
+    entries, keep, decoded_bytes, alg = [], [], 0, 0
+    plans = []
+    for k in range(n):
+        w, h = frames[k][1], frames[k][2]
+        s = 2 if types[k] == 1 else 4
+        st, meta = api.parse_metadata(files[k])
+        assert st == Status.success
+        src_dev = torch.from_numpy(np.frombuffer(files[k], dtype=np.uint8).copy()).cuda()
+        pitch = (w * s + 127) // 128 * 128
+        out = torch.empty(pitch * h, dtype=torch.uint8, device="cuda")
+        src = CompressedInput()
+        src.bytes = ConstBytes(src_dev.data_ptr(), len(files[k]))
+        src.metadata = meta.handle
+        item = BatchItem()
+        item.compressed_input = src
+        item.output = api.view(out, int(types[k]), w, h, pitch)
+        entries.append((cuda.Operation.decompress, item))
+        keep += [meta, src_dev, out]
+        decoded_bytes += w * h * s
+        t = meta.tiles
+        alg += int(t["length"].sum()) + 32 * len(t) + w * h * s
+        st, plan = cuda.prepare_batch(cuda.make_request(cuda.Operation.decompress, [item]),
+                                      None, stream)
+        assert st == Status.success
+        plans.append((plan, out, pitch, w, h, s))
+    results = torch.zeros(16 * n, dtype=torch.uint8, device="cuda")
+    t0 = time.perf_counter()
+    st, batch = cuda.prepare_mixed_batch(entries, results, stream, graph=True, autotune=True)
+    prepare_s = time.perf_counter() - t0
+    assert st == Status.success, st
+    assert batch.run(stream) == Status.success
+    torch.cuda.synchronize()
+    exact = True
+    for k, (plan, out, pitch, w, h, s) in enumerate(plans):
+        rows = out.view(h, pitch)[:, :w * s]
+        exact = exact and bool(torch.equal(rows, frames[k][0].view(h, w * s)))
+    recs = results.cpu().numpy().view(np.uint64).reshape(-1, 2)
+    exact = exact and bool(np.all(recs[:, 0] == 0))
+    steps = max(3, args.steps // 300)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(args.warmup):
+        batch.run(stream)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(steps):
+        batch.run(stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    batched_ms = e0.elapsed_time(e1) / steps
+
+    ws = torch.empty(max(max(p[0].workspace_bytes() for p in plans), 256), dtype=torch.uint8,
+                     device="cuda")
+    res1 = torch.zeros(16, dtype=torch.uint8, device="cuda")
+
+    def per_image():
+        for plan, *_ in plans:
+            cuda.decompress_async(plan, ws, res1, stream)
+
+    per_image()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(steps):
+        per_image()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    eager_ms = e0.elapsed_time(e1) / steps
+    graphed_ms = time_graph(torch, stream, per_image, steps, args.warmup)
+    return {"workload": f"{n} archives, width/height uniform 257..4096, 70% uint16 / 30% "
+                        "float32, random tile geometry, pitched output rows, whole-image decode",
+            "decoded_bytes": decoded_bytes,
+            "batched": {"ms": round(batched_ms, 4),
+                        "decoded_gbs": round(decoded_bytes / batched_ms / 1e6, 1),
+                        "roofline_frac": round(alg / batched_ms / 1e6 / peak, 4),
+                        "hbm_gbs": round(alg / batched_ms / 1e6, 1),
+                        "kernel_launches": 1, "prepare_s": round(prepare_s, 3),
+                        **batch.stats()},
+            "per_image_eager": {"ms": round(eager_ms, 4),
+                                "decoded_gbs": round(decoded_bytes / eager_ms / 1e6, 1),
+                                "kernel_launches": n},
+            "per_image_graph": {"ms": round(graphed_ms, 4),
+                                "decoded_gbs": round(decoded_bytes / graphed_ms / 1e6, 1)},
+            "speedup_vs_per_image_eager": round(eager_ms / batched_ms, 2),
+            "speedup_vs_per_image_graph": round(graphed_ms / batched_ms, 2),
+            "bit_exact": exact}
+
+
 def run_profile_case(kind: str, launches: int = 3):
     """A small case for ncu captures: one launch of `kind` over four 4096x4096 frames (about
     216 MB of decode traffic, more than the 126 MB L2), repeated `launches` times."""
@@ -495,6 +740,9 @@ def main():
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--copies", type=int, default=4)
     p.add_argument("--cpu-seconds", type=float, default=10.0)
+    p.add_argument("--sections", default="calibrated,batched",
+                   help="extra configs reported beside the headline (comma list, or none)")
+    p.add_argument("--archives", type=int, default=256, help="archives of the batched config")
     args = p.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -519,6 +767,13 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     line, shapes = run_ours(args, rank, world, local, torch, dist)
     if rank == 0:
+        sections = [s for s in args.sections.split(",") if s and s != "none"]
+        stream = torch.cuda.current_stream()
+        peak = measured_peaks()[0]
+        if "calibrated" in sections:
+            line["calibrated_decode"] = run_calibrated(args, torch, stream, peak)
+        if "batched" in sections:
+            line["batched_decode"] = run_batched(args, torch, stream, peak)
         line["cpu_baseline"] = cpu_baseline(shapes, args.cpu_seconds)
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -126,6 +126,32 @@ int ts_calibrate_async(const ts_plan *plan, ts_mutable_bytes workspace, ts_resul
 int ts_decode_calibrate_async(const ts_plan *plan, ts_mutable_bytes workspace,
                               ts_result_buffer results, void *stream);
 
+/* ---- mixed batches (include/tilestream/batch.h; extension, no reference counterpart) -------
+ * Many archives and ROIs with mixed pixel types, tile geometries and decode operations in one
+ * persistent kernel over one device task queue, replayed as a CUDA graph, optionally tuned. */
+typedef struct {
+    uint32_t operation; /* 1 decompress, 2 decode_roi, 4 decode_calibrate */
+    ts_batch_item item;
+} ts_mixed_item; /* MixedItem */
+typedef struct {
+    uint32_t graph;         /* nonzero: executions replay a CUDA graph */
+    uint32_t autotune;      /* nonzero: time candidate kernel shapes and grids at preparation */
+    const char *tune_cache; /* file remembering tuned choices, or NULL */
+} ts_mixed_options;
+typedef struct {
+    uint64_t tiles;
+    uint32_t shape, grid, per_sm, graph;
+    float tuned_us;
+} ts_mixed_stats;
+typedef struct ts_mixed_batch ts_mixed_batch;
+
+/* Results: one record per item, bound at preparation. *batch is replaced only on success. */
+int ts_prepare_mixed_batch(const ts_mixed_item *items, uint64_t count, ts_result_buffer results,
+                           const ts_mixed_options *options, ts_mixed_batch **batch, void *stream);
+int ts_run_mixed_batch(const ts_mixed_batch *batch, void *stream);
+int ts_mixed_batch_stats(const ts_mixed_batch *batch, ts_mixed_stats *stats);
+void ts_mixed_batch_destroy(ts_mixed_batch *batch);
+
 /* ---- allocation-free encode (no counterpart in the reference) ------------------------------
  * Encodes one image into a complete .tsc file on the GPU, like a one-item compress plan, but
  * allocates no memory: no plan tables, no workspace, no cudaMalloc or cudaFree. It is for

@@ -109,6 +109,19 @@ class ResultBuffer(C.Structure):
     _fields_ = [("data", vp), ("count", u64)]
 
 
+class MixedItem(C.Structure):
+    _fields_ = [("operation", u32), ("item", BatchItem)]
+
+
+class MixedOptions(C.Structure):
+    _fields_ = [("graph", u32), ("autotune", u32), ("tune_cache", C.c_char_p)]
+
+
+class MixedStats(C.Structure):
+    _fields_ = [("tiles", u64), ("shape", u32), ("grid", u32), ("per_sm", u32), ("graph", u32),
+                ("tuned_us", C.c_float)]
+
+
 _SIGNATURES = {
     "ts_image_span": (C.c_int, [ImageSpec, u64, C.POINTER(u64)]),
     "ts_compress_bound": (C.c_int, [ImageSpec, TileShape, C.POINTER(u64)]),
@@ -131,6 +144,11 @@ _SIGNATURES = {
     "ts_decode_roi_async": (C.c_int, [vp, MutableBytes, ResultBuffer, vp]),
     "ts_calibrate_async": (C.c_int, [vp, MutableBytes, ResultBuffer, vp]),
     "ts_decode_calibrate_async": (C.c_int, [vp, MutableBytes, ResultBuffer, vp]),
+    "ts_prepare_mixed_batch": (C.c_int, [C.POINTER(MixedItem), u64, ResultBuffer,
+                                         C.POINTER(MixedOptions), C.POINTER(vp), vp]),
+    "ts_run_mixed_batch": (C.c_int, [vp, vp]),
+    "ts_mixed_batch_stats": (C.c_int, [vp, C.POINTER(MixedStats)]),
+    "ts_mixed_batch_destroy": (None, [vp]),
     "ts_compress_noalloc": (C.c_int, [ConstImageView, TileShape, MutableBytes, vp, vp]),
     "ts_compress_noalloc_max_tiles": (u64, []),
     "ts_device_allocate": (C.c_int, [u64, vp, C.POINTER(vp)]),

@@ -1,4 +1,5 @@
 // The C entry layer of include/tilestream_c.h over the C++ API.
+#include <tilestream/batch.h>
 #include <tilestream/cpu.h>
 #include <tilestream/cuda.h>
 #include <tilestream/info.h>
@@ -50,8 +51,16 @@ static_assert(sizeof(ts::cuda::DeviceTile) == 40 && sizeof(ts::cuda::DeviceSegme
 static_assert(std::is_trivially_copyable_v<ts::cuda::DeviceImage> &&
               std::is_standard_layout_v<ts::cuda::DeviceBatch>);
 
+TS_SAME_LAYOUT(ts_mixed_item, ts::cuda::MixedItem);
+TS_SAME_LAYOUT(ts_mixed_stats, ts::cuda::MixedStats);
+static_assert(offsetof(ts_mixed_item, item) == offsetof(ts::cuda::MixedItem, item));
+
 struct ts_metadata {
     ts::ImageMetadata value;
+};
+
+struct ts_mixed_batch {
+    std::unique_ptr<ts::cuda::MixedBatch> batch;
 };
 
 struct ts_plan {
@@ -279,6 +288,61 @@ int ts_info_json(char *buf, uint64_t capacity, uint64_t *needed) {
 }
 
 } // extern "C"
+
+extern "C" int ts_prepare_mixed_batch(const ts_mixed_item *items, uint64_t count,
+                                      ts_result_buffer results, const ts_mixed_options *options,
+                                      ts_mixed_batch **batch, void *stream) {
+    if (batch == nullptr || (count != 0 && items == nullptr)) {
+        return code(ts::Status::invalid_argument);
+    }
+    if (count > UINT32_MAX) {
+        return code(ts::Status::resource_limit);
+    }
+    try {
+        std::vector<ts::cuda::MixedItem> converted(count);
+        for (uint64_t i = 0; i < count; ++i) {
+            converted[i] = as<ts::cuda::MixedItem>(items[i]);
+            const ts_metadata *m = items[i].item.compressed_input.metadata;
+            converted[i].item.compressed_input.metadata = m != nullptr ? &m->value : nullptr;
+        }
+        ts::cuda::MixedOptions o;
+        if (options != nullptr) {
+            o.graph = options->graph != 0;
+            o.autotune = options->autotune != 0;
+            o.tune_cache = options->tune_cache;
+        }
+        auto holder = std::make_unique<ts_mixed_batch>();
+        const ts::Status st = ts::cuda::prepare_mixed_batch(
+            converted.data(), count, as<ts::cuda::ResultBuffer>(results), o, holder->batch,
+            stream_of(stream));
+        if (st == ts::Status::success) {
+            delete *batch;
+            *batch = holder.release();
+        }
+        return code(st);
+    } catch (...) {
+        return code(ts::Status::resource_limit);
+    }
+}
+
+extern "C" int ts_run_mixed_batch(const ts_mixed_batch *batch, void *stream) {
+    if (batch == nullptr || !batch->batch) {
+        return code(ts::Status::invalid_argument);
+    }
+    return code(ts::cuda::run_mixed_batch(*batch->batch, stream_of(stream)));
+}
+
+extern "C" int ts_mixed_batch_stats(const ts_mixed_batch *batch, ts_mixed_stats *stats) {
+    if (batch == nullptr || !batch->batch || stats == nullptr) {
+        return code(ts::Status::invalid_argument);
+    }
+    *stats = as<ts_mixed_stats>(ts::cuda::mixed_batch_stats(*batch->batch));
+    return 0;
+}
+
+extern "C" void ts_mixed_batch_destroy(ts_mixed_batch *batch) {
+    delete batch;
+}
 
 // Allocation-free one-image encode (declared in include/tilestream_c.h; no counterpart in the
 // reference). Host checks follow compress_async's (draft_compress and check_execution in

@@ -10,6 +10,12 @@
 // reference's per-window bound, so workspace_size() callers allocate what they always did.
 #include "plan.h"
 
+#include <tilestream/batch.h>
+
+#include <map>
+#include <mutex>
+#include <string>
+
 #include <algorithm>
 #include <cstdio>
 #include <cstdlib>
@@ -148,6 +154,7 @@ struct Draft {
     std::vector<tsk_decode_task> tasks;
     std::vector<tsk_row_start> rows;
     bool trusted = false;
+    bool any_u16 = false, any_f32 = false, any_plain = false, any_calibrated = false;
 
     std::vector<tsk_encode_image> encode_images;
     std::uint64_t total_tiles = 0;
@@ -452,11 +459,13 @@ Status stage_tiles(const CompressedInput &src, const Roi &roi, std::uint32_t ima
     return Status::success;
 }
 
-Status draft_decode(const BatchRequest &request, Draft &d) {
-    bool mixed = false;
-    const bool calibrated = request.operation == Operation::decode_calibrate;
-    for (std::uint64_t i = 0; i < request.count; ++i) {
-        const BatchItem &item = request.items[i];
+// Validates and plans one decode item (reference plan.cpp:351-460 per item). With one_type the
+// item must have the batch's pixel type (the reference API's rule for one batch); the mixed
+// batch API lifts it.
+Status draft_decode_item(const BatchItem &item, Operation operation, bool first, bool one_type,
+                         Draft &d, bool &mixed) {
+    const bool calibrated = operation == Operation::decode_calibrate;
+    {
         const CompressedInput &src = item.compressed_input;
         const bool trusted = src.encoder_result != nullptr;
         if (trusted ? src.metadata != nullptr || src.mappings != nullptr || src.mapping_count != 0
@@ -470,13 +479,17 @@ Status draft_decode(const BatchRequest &request, Draft &d) {
         if (st != Status::success) {
             return st;
         }
-        if (i == 0) {
+        if (first) {
             d.type = image.type;
             d.shape = shape;
         }
-        if (image.type != d.type) {
+        if (one_type && image.type != d.type) {
             return Status::invalid_argument;
         }
+        d.any_u16 = d.any_u16 || image.type == PixelType::uint16;
+        d.any_f32 = d.any_f32 || image.type == PixelType::float32;
+        d.any_plain = d.any_plain || !calibrated;
+        d.any_calibrated = d.any_calibrated || calibrated;
         mixed = mixed || shape.width != d.shape.width || shape.height != d.shape.height;
         const ImageView &out = item.output;
         st = host::view_ok(out);
@@ -484,7 +497,7 @@ Status draft_decode(const BatchRequest &request, Draft &d) {
             return st;
         }
         Roi roi{0, 0, image.width, image.height};
-        if (request.operation != Operation::decompress) {
+        if (operation != Operation::decompress) {
             roi = item.roi;
             if (roi.width == 0 || roi.height == 0 ||
                 std::uint64_t{roi.x} + roi.width > image.width ||
@@ -580,6 +593,18 @@ Status draft_decode(const BatchRequest &request, Draft &d) {
         d.pointers.push_back(src.bytes.data);
         d.pointers.push_back(out.data);
     }
+    return Status::success;
+}
+
+Status draft_decode(const BatchRequest &request, Draft &d) {
+    bool mixed = false;
+    for (std::uint64_t i = 0; i < request.count; ++i) {
+        const Status st = draft_decode_item(request.items[i], request.operation, i == 0, true, d,
+                                            mixed);
+        if (st != Status::success) {
+            return st;
+        }
+    }
     if (mixed) {
         d.shape = {64, 64}; // the geometry with the most rows bounds every window
     }
@@ -641,6 +666,8 @@ std::uint32_t decode_shape() {
     return shape;
 }
 
+Status finalize(Operation operation, Draft &d, PlanState &plan, cudaStream_t stream);
+
 Status build(const BatchRequest &request, PlanState &plan, cudaStream_t stream) {
     plan.operation = request.operation;
     plan.count = request.count;
@@ -648,12 +675,19 @@ Status build(const BatchRequest &request, PlanState &plan, cudaStream_t stream) 
         return Status::success;
     }
     Draft d;
-    Status st = request.operation == Operation::compress    ? draft_compress(request, d)
-                : request.operation == Operation::calibrate ? draft_calibrate(request, d)
-                                                            : draft_decode(request, d);
+    const Status st = request.operation == Operation::compress    ? draft_compress(request, d)
+                      : request.operation == Operation::calibrate ? draft_calibrate(request, d)
+                                                                  : draft_decode(request, d);
     if (st != Status::success) {
         return st;
     }
+    return finalize(request.operation, d, plan, stream);
+}
+
+// Everything after the host-side draft: aliasing, device and pointer checks, the reported
+// workspace spec, device tables, kernel preload and upload (reference plan.cpp:516-623).
+Status finalize(Operation operation, Draft &d, PlanState &plan, cudaStream_t stream) {
+    Status st = Status::success;
     plan.type = d.type;
     if (!plan.ranges.assign(std::move(d.writable), std::move(d.readable))) {
         return Status::invalid_argument;
@@ -677,10 +711,10 @@ Status build(const BatchRequest &request, PlanState &plan, cudaStream_t stream) 
     }
 
     plan.spec = {0, 0, d.shape, 0};
-    if (request.operation != Operation::calibrate) {
+    if (operation != Operation::calibrate) {
         window_spec(d.tiles_per_image, plan.spec);
     }
-    if (request.operation == Operation::compress) {
+    if (operation == Operation::compress) {
         // This encoder's own device-wide primitive: the look-back flags of every tile.
         plan.spec.scan_temp_bytes = tsk_encode_state_bytes(d.total_tiles);
     }
@@ -718,7 +752,7 @@ Status build(const BatchRequest &request, PlanState &plan, cudaStream_t stream) 
 
     // Load every kernel the plan launches now, so no execution has to (docs/api.md:69).
     int err = 0;
-    switch (request.operation) {
+    switch (operation) {
     case Operation::compress:
         err = tsk_encode_prepare(plan.device);
         break;
@@ -726,11 +760,10 @@ Status build(const BatchRequest &request, PlanState &plan, cudaStream_t stream) 
         err = tsk_calibrate_prepare(plan.device);
         break;
     default:
-        // One pixel type per reference batch; the calibrated operation is the fused path.
-        plan.config.paths =
-            (d.type == PixelType::float32 ? TSK_PATH_F32 : TSK_PATH_U16) |
-            (request.operation == Operation::decode_calibrate ? TSK_PATH_CALIBRATED
-                                                              : TSK_PATH_PLAIN);
+        // The kernel instance carries only the paths the plan's tiles need.
+        plan.config.paths = (d.any_u16 ? TSK_PATH_U16 : 0) | (d.any_f32 ? TSK_PATH_F32 : 0) |
+                            (d.any_plain ? TSK_PATH_PLAIN : 0) |
+                            (d.any_calibrated ? TSK_PATH_CALIBRATED : 0);
         plan.config.shape = decode_shape();
         err = tsk_decode_prepare(&plan.config, plan.task_count, plan.device);
         break;
@@ -898,6 +931,290 @@ Status calibrate_async(const BatchPlan &plan, MutableBytes workspace, ResultBuff
     return detail::cuda_status(tsk_calibrate_launch(
         p->calib_tasks, p->calib_task_count, p->calib_images, static_cast<std::uint32_t>(p->count),
         reinterpret_cast<tsk_result *>(results.data), stream), "calibrate launch");
+}
+
+// ---- mixed batches (include/tilestream/batch.h) ---------------------------------------------
+
+struct MixedBatch::Impl {
+    detail::PlanState plan;
+    tsk_result *results = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    MixedStats stats;
+
+    ~Impl() {
+        if (exec != nullptr) {
+            static_cast<void>(cudaGraphExecDestroy(exec));
+        }
+        if (graph != nullptr) {
+            static_cast<void>(cudaGraphDestroy(graph));
+        }
+    }
+};
+
+struct MixedAccess {
+    static MixedBatch::Impl *impl(const MixedBatch &b) noexcept {
+        return b.impl_.get();
+    }
+    static std::unique_ptr<MixedBatch> make(std::unique_ptr<MixedBatch::Impl> impl) {
+        return std::unique_ptr<MixedBatch>(new MixedBatch(std::move(impl)));
+    }
+};
+
+MixedBatch::MixedBatch(std::unique_ptr<Impl> impl) noexcept : impl_(std::move(impl)) {}
+MixedBatch::~MixedBatch() = default;
+
+namespace {
+
+// One eager execution of a decode plan (used by executions without a graph and by the tuner).
+cudaError_t enqueue_decode(const detail::PlanState &p, tsk_result *results, cudaStream_t stream) {
+    if (p.trusted) {
+        const cudaError_t e =
+            cudaMemsetAsync(results, 0, sizeof(tsk_result) * p.count, stream);
+        if (e != cudaSuccess) return e;
+    }
+    return static_cast<cudaError_t>(tsk_decode_launch(p.tasks, p.task_count, p.images, p.rows,
+                                                      results, p.config, stream));
+}
+
+// The tuner's memory: workload key -> (shape, resident CTAs per SM).
+struct TuneChoice {
+    std::uint32_t shape = 0, per_sm = 0;
+};
+std::mutex g_tune_mutex;
+std::map<std::string, TuneChoice> g_tune_memo;
+
+std::string tune_key(const detail::PlanState &p, int device) {
+    cudaDeviceProp prop{};
+    static_cast<void>(cudaGetDeviceProperties(&prop, device));
+    // The workload signature: device, kernel paths and the task count rounded to a power of two.
+    std::uint32_t order = 0;
+    while ((1ull << order) < p.task_count) {
+        ++order;
+    }
+    std::string key = prop.name;
+    for (char &c : key) {
+        if (c == ' ') c = '_';
+    }
+    return key + "/paths" + std::to_string(p.config.paths) + "/tasks2^" + std::to_string(order);
+}
+
+void load_tune_cache(const char *path) {
+    if (path == nullptr) return;
+    std::FILE *f = std::fopen(path, "r");
+    if (f == nullptr) return;
+    char key[512];
+    unsigned shape = 0, per_sm = 0;
+    while (std::fscanf(f, "%511s %u %u", key, &shape, &per_sm) == 3) {
+        g_tune_memo[key] = {shape, per_sm};
+    }
+    std::fclose(f);
+}
+
+void save_tune_cache(const char *path) {
+    if (path == nullptr) return;
+    std::FILE *f = std::fopen(path, "w");
+    if (f == nullptr) return;
+    for (const auto &[key, c] : g_tune_memo) {
+        std::fprintf(f, "%s %u %u\n", key.c_str(), c.shape, c.per_sm);
+    }
+    std::fclose(f);
+}
+
+// Times candidate configurations (kernel shape x resident CTAs per SM) on the real batch and
+// keeps the fastest. Every candidate writes the same outputs and results.
+Status autotune(detail::PlanState &p, tsk_result *results, const char *cache, cudaStream_t stream,
+                float &best_us) {
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    load_tune_cache(cache);
+    const std::string key = tune_key(p, p.device);
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p.device) != cudaSuccess) {
+        return detail::cuda_failure("cudaDeviceGetAttribute");
+    }
+    auto apply = [&](std::uint32_t shape, std::uint32_t per_sm) -> cudaError_t {
+        tsk_decode_config c = p.config;
+        c.shape = shape;
+        const int e = tsk_decode_prepare(&c, p.task_count, p.device);
+        if (e != 0) return static_cast<cudaError_t>(e);
+        const std::uint32_t k = per_sm == 0 || per_sm > c.per_sm ? c.per_sm : per_sm;
+        const std::uint64_t grid = static_cast<std::uint64_t>(sms) * k;
+        c.grid = static_cast<std::uint32_t>(std::max<std::uint64_t>(
+            1, std::min<std::uint64_t>(grid, p.task_count)));
+        c.per_sm = k;
+        p.config = c;
+        return cudaSuccess;
+    };
+    const auto hit = g_tune_memo.find(key);
+    if (hit != g_tune_memo.end()) {
+        return detail::cuda_status(apply(hit->second.shape, hit->second.per_sm), "tuned config");
+    }
+    const bool plain_u16 = p.config.paths == (TSK_PATH_U16 | TSK_PATH_PLAIN);
+    const std::uint32_t shapes_all[] = {0, 1, 2, 3}, shapes_two[] = {0, 2};
+    const std::uint32_t *shapes = plain_u16 ? shapes_all : shapes_two;
+    const std::size_t nshapes = plain_u16 ? 4 : 2;
+    cudaEvent_t start = nullptr, stop = nullptr;
+    if (cudaEventCreate(&start) != cudaSuccess || cudaEventCreate(&stop) != cudaSuccess) {
+        return detail::cuda_failure("cudaEventCreate");
+    }
+    TuneChoice best;
+    best_us = 0.0f;
+    cudaError_t e = cudaSuccess;
+    for (std::size_t i = 0; i < nshapes && e == cudaSuccess; ++i) {
+        tsk_decode_config probe = p.config;
+        probe.shape = shapes[i];
+        e = static_cast<cudaError_t>(tsk_decode_prepare(&probe, p.task_count, p.device));
+        for (std::uint32_t k = probe.per_sm; k >= 1 && e == cudaSuccess; --k) {
+            e = apply(shapes[i], k);
+            if (e == cudaSuccess) e = enqueue_decode(p, results, stream); // warm-up
+            constexpr int kRuns = 3;
+            if (e == cudaSuccess) e = cudaEventRecord(start, stream);
+            for (int r = 0; r < kRuns && e == cudaSuccess; ++r) {
+                e = enqueue_decode(p, results, stream);
+            }
+            if (e == cudaSuccess) e = cudaEventRecord(stop, stream);
+            if (e == cudaSuccess) e = cudaEventSynchronize(stop);
+            float ms = 0.0f;
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, start, stop);
+            const float us = ms * 1000.0f / kRuns;
+            if (e == cudaSuccess && (best_us == 0.0f || us < best_us)) {
+                best_us = us;
+                best = {shapes[i], k};
+            }
+            if (k + 2 < probe.per_sm) {
+                break; // fewer CTAs than that never won on this kernel
+            }
+        }
+    }
+    cudaEventDestroy(start);
+    cudaEventDestroy(stop);
+    if (e != cudaSuccess) {
+        return detail::cuda_failure("autotune", e);
+    }
+    g_tune_memo[key] = best;
+    save_tune_cache(cache);
+    return detail::cuda_status(apply(best.shape, best.per_sm), "tuned config");
+}
+
+} // namespace
+
+Status prepare_mixed_batch(const MixedItem *items, std::uint64_t count, ResultBuffer results,
+                           const MixedOptions &options, std::unique_ptr<MixedBatch> &batch,
+                           cudaStream_t stream) noexcept {
+    if (count > UINT32_MAX) {
+        return Status::resource_limit;
+    }
+    if (count != 0 && items == nullptr) {
+        return Status::invalid_argument;
+    }
+    try {
+        auto impl = std::make_unique<MixedBatch::Impl>();
+        detail::PlanState &plan = impl->plan;
+        plan.operation = Operation::decode_roi;
+        plan.count = count;
+        if (count != 0) {
+            detail::Draft d;
+            bool mixed = false;
+            for (std::uint64_t i = 0; i < count; ++i) {
+                const Operation op = items[i].operation;
+                if (op != Operation::decompress && op != Operation::decode_roi &&
+                    op != Operation::decode_calibrate) {
+                    return Status::invalid_argument;
+                }
+                const Status st = detail::draft_decode_item(items[i].item, op, i == 0, false, d,
+                                                            mixed);
+                if (st != Status::success) {
+                    return st;
+                }
+            }
+            if (mixed) {
+                d.shape = {64, 64};
+            }
+            std::uint64_t result_bytes = 0;
+            if (!host::mul(results.count, sizeof(DeviceResult), result_bytes)) {
+                return Status::size_overflow;
+            }
+            Status st = host::byte_range(results.data, result_bytes);
+            if (st != Status::success) {
+                return st;
+            }
+            if (results.count < count) {
+                return Status::buffer_too_small;
+            }
+            if (reinterpret_cast<std::uintptr_t>(results.data) % alignof(DeviceResult) != 0) {
+                return Status::invalid_argument;
+            }
+            d.writable.push_back(detail::range_of(results.data, result_bytes));
+            d.pointers.push_back(results.data);
+            st = detail::finalize(Operation::decode_roi, d, plan, stream);
+            if (st != Status::success) {
+                return st;
+            }
+            impl->results = reinterpret_cast<tsk_result *>(results.data);
+            if (options.autotune) {
+                const char *cache = options.tune_cache != nullptr
+                                        ? options.tune_cache
+                                        : std::getenv("TILESTREAM_TUNE_CACHE");
+                st = autotune(plan, impl->results, cache, stream, impl->stats.tuned_us);
+                if (st != Status::success) {
+                    return st;
+                }
+            }
+            if (options.graph) {
+                const int e = tsk_decode_graph(plan.tasks, plan.task_count, plan.images, plan.rows,
+                                               impl->results, static_cast<std::uint32_t>(count),
+                                               plan.trusted ? 1 : 0, plan.config, &impl->graph,
+                                               &impl->exec);
+                if (e != 0) {
+                    impl->graph = nullptr;
+                    impl->exec = nullptr;
+                    return detail::cuda_failure("graph instantiation",
+                                                static_cast<cudaError_t>(e));
+                }
+                // Upload the graph now so that the first execution does no set-up work.
+                if (cudaGraphUpload(impl->exec, stream) != cudaSuccess ||
+                    cudaStreamSynchronize(stream) != cudaSuccess) {
+                    return detail::cuda_failure("cudaGraphUpload");
+                }
+            }
+            impl->stats = {plan.task_count, plan.config.shape, plan.config.grid,
+                           plan.config.per_sm, impl->exec != nullptr ? 1u : 0u,
+                           impl->stats.tuned_us};
+        }
+        batch = MixedAccess::make(std::move(impl));
+        return Status::success;
+    } catch (const std::bad_alloc &) {
+        return Status::resource_limit;
+    } catch (const std::length_error &) {
+        return Status::resource_limit;
+    }
+}
+
+Status run_mixed_batch(const MixedBatch &batch, cudaStream_t stream) noexcept {
+    const MixedBatch::Impl *impl = MixedAccess::impl(batch);
+    if (impl == nullptr) {
+        return Status::invalid_argument;
+    }
+    const detail::PlanState &p = impl->plan;
+    if (p.count == 0) {
+        return Status::success;
+    }
+    Status st = detail::stream_device(stream, p.device);
+    if (st == Status::success && cudaPeekAtLastError() != cudaSuccess) {
+        st = Status::cuda_error; // left for the caller
+    }
+    if (st != Status::success) {
+        return st;
+    }
+    if (impl->exec != nullptr) {
+        return detail::cuda_status(cudaGraphLaunch(impl->exec, stream), "cudaGraphLaunch");
+    }
+    return detail::cuda_status(enqueue_decode(p, impl->results, stream), "decode launch");
+}
+
+MixedStats mixed_batch_stats(const MixedBatch &batch) noexcept {
+    const MixedBatch::Impl *impl = MixedAccess::impl(batch);
+    return impl != nullptr ? impl->stats : MixedStats{};
 }
 
 } // namespace tilestream::cuda

@@ -753,8 +753,12 @@ Variant make() {
             sizeof(Shared<MaxPayload, Stages>), threads_of(CW)};
 }
 
+// Shapes: 0 = 8 consumer warps x 8 uint16 columns per lane, 1 = 8 x 16, 2 = 4 x 16, 3 = 4 x 8.
+// The plain uint16 instance has all four; the others have shapes 0 and 2 (odd shapes map to
+// those).
 Variant select(uint32_t paths, uint32_t shape) {
     const bool f32 = paths & kF32, u16 = paths & kU16, plain = paths & kPlain, c = paths & kCal;
+    const bool narrow = shape == 2 || shape == 3; // four consumer warps
     if (!f32) {
         if (plain && !c) {
             switch (shape) {
@@ -768,14 +772,22 @@ Variant select(uint32_t paths, uint32_t shape) {
                 return make<8192, 4, kU16 | kPlain, 8, 8, 4>();
             }
         }
-        if (c && !plain) return make<8192, 4, kU16 | kCal>();
+        if (c && !plain) {
+            return narrow ? make<8192, 4, kU16 | kCal, 4, 16, 4>() : make<8192, 4, kU16 | kCal>();
+        }
         return make<8192, 4, kU16 | kPlain | kCal>();
     }
     if (!u16) {
-        if (plain && !c) return make<16384, 3, kF32 | kPlain>();
-        if (c && !plain) return make<16384, 3, kF32 | kCal>();
+        if (plain && !c) {
+            return narrow ? make<16384, 3, kF32 | kPlain, 4, 16, 4>()
+                          : make<16384, 3, kF32 | kPlain>();
+        }
+        if (c && !plain) {
+            return narrow ? make<16384, 3, kF32 | kCal, 4, 16, 4>() : make<16384, 3, kF32 | kCal>();
+        }
     }
-    return make<16384, 3, kU16 | kF32 | kPlain | kCal>();
+    return narrow ? make<16384, 3, kU16 | kF32 | kPlain | kCal, 4, 16, 4>()
+                  : make<16384, 3, kU16 | kF32 | kPlain | kCal>();
 }
 
 } // namespace
@@ -813,4 +825,49 @@ extern "C" int tsk_decode_launch(const tsk_decode_task *tasks, uint32_t ntasks,
     v.fn<<<config.grid, v.threads, v.smem, stream>>>(tasks, ntasks, images, rows, results, 1u,
                                                      0x80000000u);
     return cudaGetLastError();
+}
+
+// A CUDA graph of one execution: a clear of the result records when the plan has trusted images
+// (their completion is counted in the records), then the decode kernel node.
+extern "C" int tsk_decode_graph(const tsk_decode_task *tasks, uint32_t ntasks,
+                                const tsk_decode_image *images, const tsk_row_start *rows,
+                                tsk_result *results, uint32_t result_count, int clear_results,
+                                tsk_decode_config config, cudaGraph_t *graph_out,
+                                cudaGraphExec_t *exec_out) {
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaGraphCreate(&graph, 0);
+    if (e != cudaSuccess) return e;
+    cudaGraphNode_t clear = nullptr, kernel = nullptr;
+    if (clear_results && result_count != 0) {
+        cudaMemsetParams m{};
+        m.dst = results;
+        m.value = 0;
+        m.elementSize = 1;
+        m.width = sizeof(tsk_result) * result_count;
+        m.height = 1;
+        m.pitch = 0;
+        e = cudaGraphAddMemsetNode(&clear, graph, nullptr, 0, &m);
+    }
+    if (e == cudaSuccess && ntasks != 0) {
+        const tsk::Variant v = tsk::select(config.paths, config.shape);
+        uint32_t one = 1u, top = 0x80000000u;
+        void *args[] = {&tasks, &ntasks, &images, &rows, &results, &one, &top};
+        cudaKernelNodeParams k{};
+        k.func = reinterpret_cast<void *>(v.fn);
+        k.gridDim = dim3(config.grid);
+        k.blockDim = dim3(v.threads);
+        k.sharedMemBytes = static_cast<unsigned>(v.smem);
+        k.kernelParams = args;
+        k.extra = nullptr;
+        e = cudaGraphAddKernelNode(&kernel, graph, clear ? &clear : nullptr, clear ? 1 : 0, &k);
+    }
+    if (e == cudaSuccess) {
+        e = cudaGraphInstantiate(exec_out, graph, 0);
+    }
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        return e;
+    }
+    *graph_out = graph;
+    return cudaSuccess;
 }

@@ -153,6 +153,12 @@ int tsk_decode_launch(const tsk_decode_task *tasks, uint32_t ntasks,
                       tsk_result *results, tsk_decode_config config, cudaStream_t stream);
 // Occupancy-derived persistent grid for a decode launch, and the kernel preload.
 int tsk_decode_prepare(tsk_decode_config *config, uint32_t ntasks, int device);
+// The same execution as a CUDA graph (clear of the result records when clear_results, then the
+// kernel node), instantiated.
+int tsk_decode_graph(const tsk_decode_task *tasks, uint32_t ntasks,
+                     const tsk_decode_image *images, const tsk_row_start *rows,
+                     tsk_result *results, uint32_t result_count, int clear_results,
+                     tsk_decode_config config, cudaGraph_t *graph, cudaGraphExec_t *exec);
 
 // Encodes every tile of every image in one pass. state: 8 * (total_tiles + 2) bytes of
 // workspace, cleared by the launcher in stream order.

@@ -120,3 +120,43 @@ def allocate(nbytes: int, stream=None):
 
 def release(address: int, stream=None) -> Status:
     return Status(N.lib().ts_device_release(address, stream_handle(stream)))
+
+
+# ---- mixed batches (include/tilestream/batch.h) ----------------------------------------------
+
+class MixedBatch:
+    """An owned tilestream::cuda::MixedBatch: many decodes of mixed pixel types, geometries and
+    operations in one persistent kernel, replayed as a CUDA graph."""
+
+    def __init__(self, handle: int, keep=()):
+        self.handle = handle
+        self._keep = keep
+
+    def run(self, stream=None) -> Status:
+        return Status(N.lib().ts_run_mixed_batch(self.handle, stream_handle(stream)))
+
+    def stats(self) -> dict:
+        s = N.MixedStats()
+        N.lib().ts_mixed_batch_stats(self.handle, C.byref(s))
+        return {"tiles": s.tiles, "shape": s.shape, "grid": s.grid, "per_sm": s.per_sm,
+                "graph": bool(s.graph), "tuned_us": round(s.tuned_us, 2)}
+
+    def __del__(self):
+        if getattr(self, "handle", None):
+            N.lib().ts_mixed_batch_destroy(self.handle)
+            self.handle = None
+
+
+def prepare_mixed_batch(items, results, stream=None, graph=True, autotune=False,
+                        tune_cache=None):
+    """items: iterable of (Operation, BatchItem). Returns (Status, MixedBatch or None)."""
+    items = list(items)
+    arr = (N.MixedItem * max(1, len(items)))(*[N.MixedItem(int(op), it) for op, it in items])
+    opts = N.MixedOptions(1 if graph else 0, 1 if autotune else 0,
+                          tune_cache.encode() if tune_cache else None)
+    h = C.c_void_p(0)
+    st = N.lib().ts_prepare_mixed_batch(arr, len(items), _results(results), C.byref(opts),
+                                        C.byref(h), stream_handle(stream))
+    if st == 0:
+        return Status.success, MixedBatch(h.value)
+    return Status(st), None
