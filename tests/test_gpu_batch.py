@@ -60,7 +60,14 @@ def verify(checks, results):
     for k, (out, pitch, row_bytes, rh, want, nbytes) in enumerate(checks):
         assert int(raw[k, 0]) == 0 and int(raw[k, 1]) == nbytes, k
         got = host(out)[:pitch * rh].reshape(rh, pitch)
-        assert np.array_equal(got[:, :row_bytes], want), k
+        rows = np.ascontiguousarray(got[:, :row_bytes])
+        if nbytes == rh * row_bytes and (k % 3) == 2:
+            # Calibrated FP32: bit-exact except NaN payloads (NaNs compare by class).
+            a, b = rows.view(np.float32), np.ascontiguousarray(want).view(np.float32)
+            assert np.all((a.view(np.uint32) == b.view(np.uint32)) |
+                          (np.isnan(a) & np.isnan(b))), k
+        else:
+            assert np.array_equal(rows, want), k
         assert np.all(got[:, row_bytes:] == SENTINEL), k
 
 
