@@ -671,6 +671,80 @@ def run_batched(args, torch, stream, peak):
             "bit_exact": exact}
 
 
+def serve_summary(stats, count):
+    return {"requests": count, "completed": stats.completed,
+            "p50_ms": round(stats.p50_us / 1e3, 4), "p90_ms": round(stats.p90_us / 1e3, 4),
+            "p99_ms": round(stats.p99_us / 1e3, 4), "max_ms": round(stats.max_us / 1e3, 4),
+            "mean_ms": round(stats.mean_us / 1e3, 4),
+            "throughput_rps": round(stats.throughput_rps, 1),
+            "decoded_gbs": round(stats.decoded_gbs, 2), "wall_s": round(stats.wall_us / 1e6, 4),
+            "launches": stats.batches, "mean_batch": round(stats.mean_batch, 3),
+            "max_inflight": stats.max_inflight, "stalls": stats.stalls, "tiles": stats.tiles}
+
+
+def run_serving(args, torch, stream):
+    """Config 5: 64 uint16 8192x8192 archives with 64x64 tiles resident in device memory; a
+    request stream with Poisson arrivals at 20k req/s, each an ROI with sides log-uniform in
+    32..4096 px at a uniform offset, 40% with fused scalar calibration (offset 100.0, gain 1.05).
+    Continuous batching against one request at a time (resident tables, and the plan API)."""
+    from tilestream_b200 import api, cuda, workloads
+    from tilestream_b200.api import ConstBytes, Status
+    n, side, tile = args.serve_archives, 8192, (64, 64)
+    files = []
+    for g in range(0, n, 8):
+        frames = [workloads.detector_frame_torch(side, side, 5000 + k).view(torch.uint8)
+                  .reshape(-1).contiguous() for k in range(g, min(n, g + 8))]
+        files += encode_on_gpu(torch, stream, [(f, side, side, side * 2) for f in frames], 1,
+                               tile)
+        del frames
+    resident, metas, compressed = [], [], 0
+    for f in files:
+        st, meta = api.parse_metadata(f)
+        assert st == Status.success, st
+        dev = torch.from_numpy(np.frombuffer(f, dtype=np.uint8).copy()).cuda()
+        resident.append(dev)
+        metas.append(meta)
+        compressed += len(f)
+    del files
+    rate = args.serve_rate
+    stream_arrays = workloads.serving_requests(args.serve_requests, n, side, side, rate, seed=5)
+    requests = cuda.serve_requests(stream_arrays)
+    serial_count = min(len(requests), args.serve_serial_requests)
+    serial_requests = (cuda.N.ServeRequest * serial_count)(*requests[:serial_count])
+    warm = workloads.serving_requests(200, n, side, side, rate, seed=6)
+    results = {}
+    for name, options, reqs in (
+            ("continuous_batching", dict(max_batch=48, max_inflight=4), requests),
+            ("one_at_a_time_resident", dict(max_batch=1, max_inflight=1), requests),
+            ("one_at_a_time_plan", dict(serial=True), serial_requests)):
+        srv = cuda.Server(pool_bytes=args.serve_pool_gb << 30, **options)
+        for dev, meta in zip(resident, metas):
+            st, _ = srv.add_archive(ConstBytes(dev.data_ptr(), dev.numel()), meta, owner=dev)
+            assert st == Status.success, st
+        assert srv.seal() == Status.success
+        st, _, _ = srv.run(cuda.serve_requests(warm))
+        assert st == Status.success, st
+        st, outcomes, stats = srv.run(reqs)
+        assert st == Status.success, st
+        ok = all(outcomes[i].result.status == 0 for i in range(len(reqs)))
+        results[name] = {**serve_summary(stats, len(reqs)), "all_success": ok}
+        del srv
+    area = stream_arrays["width"].astype(np.float64) * stream_arrays["height"]
+    return {"workload": f"{n} uint16 {side}x{side} archives, 64x64 tiles, resident; Poisson "
+                        f"arrivals at {rate:.0f} req/s; ROI sides log-uniform 32..4096 at a "
+                        "uniform offset; 40% fused scalar calibration (offset 100.0, gain 1.05)",
+            "resident_compressed_gb": round(compressed / 1e9, 3),
+            "mean_roi_mpx": round(float(area.mean()) / 1e6, 4),
+            "calibrated_fraction": round(float(stream_arrays["calibrated"].mean()), 4),
+            "offered_gbs": round(float((area * np.where(stream_arrays["calibrated"], 4, 2))
+                                       .sum()) / (float(stream_arrays["arrival_us"][-1]) * 1e3),
+                                 2),
+            **results,
+            "p99_under_1ms": results["continuous_batching"]["p99_ms"] < 1.0,
+            "latency": "arrival (host clock, Poisson schedule) to completion seen by the "
+                       "serving loop polling the launch's event"}
+
+
 def run_profile_case(kind: str, launches: int = 3):
     """A small case for ncu captures: one launch of `kind` over four 4096x4096 frames (about
     216 MB of decode traffic, more than the 126 MB L2), repeated `launches` times."""
@@ -740,9 +814,15 @@ def main():
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--copies", type=int, default=4)
     p.add_argument("--cpu-seconds", type=float, default=10.0)
-    p.add_argument("--sections", default="calibrated,batched",
+    p.add_argument("--sections", default="calibrated,batched,serving",
                    help="extra configs reported beside the headline (comma list, or none)")
     p.add_argument("--archives", type=int, default=256, help="archives of the batched config")
+    p.add_argument("--serve-archives", type=int, default=64)
+    p.add_argument("--serve-requests", type=int, default=20000)
+    p.add_argument("--serve-serial-requests", type=int, default=2000,
+                   help="requests of the one-at-a-time plan-API baseline")
+    p.add_argument("--serve-rate", type=float, default=20000.0, help="offered requests/s")
+    p.add_argument("--serve-pool-gb", type=int, default=2)
     args = p.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -774,6 +854,8 @@ def main():
             line["calibrated_decode"] = run_calibrated(args, torch, stream, peak)
         if "batched" in sections:
             line["batched_decode"] = run_batched(args, torch, stream, peak)
+        if "serving" in sections:
+            line["serving"] = run_serving(args, torch, stream)
         line["cpu_baseline"] = cpu_baseline(shapes, args.cpu_seconds)
         print(json.dumps(line), flush=True)
     if world > 1:

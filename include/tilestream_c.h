@@ -152,6 +152,50 @@ int ts_run_mixed_batch(const ts_mixed_batch *batch, void *stream);
 int ts_mixed_batch_stats(const ts_mixed_batch *batch, ts_mixed_stats *stats);
 void ts_mixed_batch_destroy(ts_mixed_batch *batch);
 
+/* ---- ROI serving (include/tilestream/serve.h; extension, no reference counterpart) ---------
+ * Resident archives, requests admitted by output-pool memory and batched into one persistent
+ * decoder launch each, several launches in flight. Archive bytes and metadata must outlive the
+ * server. */
+typedef struct {
+    uint32_t archive;
+    ts_roi roi;
+    uint32_t calibrated; /* nonzero: FP32 output RN(RN(x - offset) * gain) */
+    float offset, gain;
+    double arrival_us; /* after the start of the run; non-decreasing */
+} ts_serve_request; /* ServeRequest */
+typedef struct {
+    uint64_t output_pool_bytes;
+    uint32_t max_batch;    /* requests per launch, 1-48 */
+    uint32_t max_inflight; /* launches on the GPU at once, 1-16 */
+    uint64_t max_batch_tiles;
+    uint32_t retain_outputs; /* nonzero: outputs stay valid until the run ends */
+    uint32_t serial;         /* nonzero: one request at a time through the plan API */
+} ts_serve_options; /* ServeOptions */
+typedef struct {
+    double wall_us, throughput_rps, decoded_gbs;
+    double p50_us, p90_us, p99_us, max_us, mean_us;
+    uint64_t completed, rejected, batches;
+    double mean_batch;
+    uint64_t max_inflight, stalls, tiles, output_bytes;
+} ts_serve_stats; /* ServeStats */
+typedef struct {
+    double latency_us, queued_us;
+    uint64_t output_offset, output_pitch;
+    uint32_t batch_size;
+    ts_device_result result;
+} ts_serve_outcome; /* ServeOutcome */
+typedef struct ts_server ts_server;
+
+/* options NULL: defaults. *server is replaced only on success. */
+int ts_server_create(const ts_serve_options *options, ts_server **server);
+int ts_server_add_archive(ts_server *server, ts_const_bytes device_bytes,
+                          const ts_metadata *metadata, uint32_t *id);
+int ts_server_seal(ts_server *server);
+int ts_server_run(ts_server *server, const ts_serve_request *requests, uint64_t count,
+                  ts_serve_outcome *outcomes, ts_serve_stats *stats);
+int ts_server_pool(const ts_server *server, ts_mutable_bytes *pool);
+void ts_server_destroy(ts_server *server);
+
 /* ---- allocation-free encode (no counterpart in the reference) ------------------------------
  * Encodes one image into a complete .tsc file on the GPU, like a one-item compress plan, but
  * allocates no memory: no plan tables, no workspace, no cudaMalloc or cudaFree. It is for

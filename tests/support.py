@@ -130,3 +130,17 @@ def crop(pixels: np.ndarray, pitch: int, s: int, roi) -> np.ndarray:
     x, y, w, h = roi
     rows = [pixels[(y + r) * pitch + x * s:(y + r) * pitch + (x + w) * s] for r in range(h)]
     return np.concatenate(rows)
+
+
+def read_device(address: int, nbytes: int) -> np.ndarray:
+    """nbytes of device memory at a raw address (memory the library owns, such as a server's
+    output pool), copied to the host through the CUDA runtime that torch has loaded."""
+    import ctypes
+    t = torch()
+    t.cuda.synchronize()
+    rt = ctypes.CDLL("libcudart.so.12")
+    out = np.empty(max(nbytes, 1), np.uint8)
+    rc = rt.cudaMemcpy(ctypes.c_void_p(out.ctypes.data), ctypes.c_void_p(address),
+                       ctypes.c_size_t(nbytes), 2)  # cudaMemcpyDeviceToHost
+    assert rc == 0, rc
+    return out[:nbytes]

@@ -122,6 +122,30 @@ class MixedStats(C.Structure):
                 ("tuned_us", C.c_float)]
 
 
+class ServeRequest(C.Structure):
+    _fields_ = [("archive", u32), ("roi", Roi), ("calibrated", u32), ("offset", C.c_float),
+                ("gain", C.c_float), ("arrival_us", C.c_double)]
+
+
+class ServeOptions(C.Structure):
+    _fields_ = [("output_pool_bytes", u64), ("max_batch", u32), ("max_inflight", u32),
+                ("max_batch_tiles", u64), ("retain_outputs", u32), ("serial", u32)]
+
+
+class ServeStats(C.Structure):
+    _fields_ = [(name, C.c_double) for name in
+                ("wall_us", "throughput_rps", "decoded_gbs", "p50_us", "p90_us", "p99_us",
+                 "max_us", "mean_us")] + \
+               [("completed", u64), ("rejected", u64), ("batches", u64),
+                ("mean_batch", C.c_double), ("max_inflight", u64), ("stalls", u64),
+                ("tiles", u64), ("output_bytes", u64)]
+
+
+class ServeOutcome(C.Structure):
+    _fields_ = [("latency_us", C.c_double), ("queued_us", C.c_double), ("output_offset", u64),
+                ("output_pitch", u64), ("batch_size", u32), ("result", DeviceResult)]
+
+
 _SIGNATURES = {
     "ts_image_span": (C.c_int, [ImageSpec, u64, C.POINTER(u64)]),
     "ts_compress_bound": (C.c_int, [ImageSpec, TileShape, C.POINTER(u64)]),
@@ -149,6 +173,13 @@ _SIGNATURES = {
     "ts_run_mixed_batch": (C.c_int, [vp, vp]),
     "ts_mixed_batch_stats": (C.c_int, [vp, C.POINTER(MixedStats)]),
     "ts_mixed_batch_destroy": (None, [vp]),
+    "ts_server_create": (C.c_int, [C.POINTER(ServeOptions), C.POINTER(vp)]),
+    "ts_server_add_archive": (C.c_int, [vp, ConstBytes, vp, C.POINTER(u32)]),
+    "ts_server_seal": (C.c_int, [vp]),
+    "ts_server_run": (C.c_int, [vp, C.POINTER(ServeRequest), u64, C.POINTER(ServeOutcome),
+                                C.POINTER(ServeStats)]),
+    "ts_server_pool": (C.c_int, [vp, C.POINTER(MutableBytes)]),
+    "ts_server_destroy": (None, [vp]),
     "ts_compress_noalloc": (C.c_int, [ConstImageView, TileShape, MutableBytes, vp, vp]),
     "ts_compress_noalloc_max_tiles": (u64, []),
     "ts_device_allocate": (C.c_int, [u64, vp, C.POINTER(vp)]),

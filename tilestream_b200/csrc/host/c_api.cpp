@@ -3,6 +3,7 @@
 #include <tilestream/cpu.h>
 #include <tilestream/cuda.h>
 #include <tilestream/info.h>
+#include <tilestream/serve.h>
 #include <tilestream_c.h>
 
 #include "plan.h"
@@ -55,6 +56,19 @@ TS_SAME_LAYOUT(ts_mixed_item, ts::cuda::MixedItem);
 TS_SAME_LAYOUT(ts_mixed_stats, ts::cuda::MixedStats);
 static_assert(offsetof(ts_mixed_item, item) == offsetof(ts::cuda::MixedItem, item));
 
+TS_SAME_LAYOUT(ts_serve_request, ts::cuda::ServeRequest);
+TS_SAME_LAYOUT(ts_serve_options, ts::cuda::ServeOptions);
+TS_SAME_LAYOUT(ts_serve_stats, ts::cuda::ServeStats);
+TS_SAME_LAYOUT(ts_serve_outcome, ts::cuda::ServeOutcome);
+static_assert(offsetof(ts_serve_request, arrival_us) ==
+              offsetof(ts::cuda::ServeRequest, arrival_us));
+static_assert(offsetof(ts_serve_options, serial) == offsetof(ts::cuda::ServeOptions, serial));
+static_assert(offsetof(ts_serve_stats, output_bytes) ==
+              offsetof(ts::cuda::ServeStats, output_bytes));
+static_assert(offsetof(ts_serve_outcome, result) == offsetof(ts::cuda::ServeOutcome, result));
+static_assert(std::is_trivially_copyable_v<ts::cuda::ServeRequest> &&
+              std::is_trivially_copyable_v<ts::cuda::ServeOutcome>);
+
 struct ts_metadata {
     ts::ImageMetadata value;
 };
@@ -65,6 +79,10 @@ struct ts_mixed_batch {
 
 struct ts_plan {
     std::unique_ptr<ts::cuda::BatchPlan> plan;
+};
+
+struct ts_server {
+    std::unique_ptr<ts::cuda::Server> server;
 };
 
 namespace {
@@ -342,6 +360,66 @@ extern "C" int ts_mixed_batch_stats(const ts_mixed_batch *batch, ts_mixed_stats 
 
 extern "C" void ts_mixed_batch_destroy(ts_mixed_batch *batch) {
     delete batch;
+}
+
+extern "C" int ts_server_create(const ts_serve_options *options, ts_server **server) {
+    if (server == nullptr) {
+        return code(ts::Status::invalid_argument);
+    }
+    try {
+        const ts::cuda::ServeOptions o =
+            options != nullptr ? as<ts::cuda::ServeOptions>(*options) : ts::cuda::ServeOptions{};
+        auto holder = std::make_unique<ts_server>();
+        const ts::Status st = ts::cuda::Server::create(o, holder->server);
+        if (st == ts::Status::success) {
+            delete *server;
+            *server = holder.release();
+        }
+        return code(st);
+    } catch (...) {
+        return code(ts::Status::resource_limit);
+    }
+}
+
+extern "C" int ts_server_add_archive(ts_server *server, ts_const_bytes device_bytes,
+                                     const ts_metadata *metadata, uint32_t *id) {
+    if (server == nullptr || !server->server || metadata == nullptr || id == nullptr) {
+        return code(ts::Status::invalid_argument);
+    }
+    return code(server->server->add_archive(as<ts::ConstBytes>(device_bytes), metadata->value,
+                                            *id));
+}
+
+extern "C" int ts_server_seal(ts_server *server) {
+    if (server == nullptr || !server->server) {
+        return code(ts::Status::invalid_argument);
+    }
+    return code(server->server->seal());
+}
+
+extern "C" int ts_server_run(ts_server *server, const ts_serve_request *requests, uint64_t count,
+                             ts_serve_outcome *outcomes, ts_serve_stats *stats) {
+    if (server == nullptr || !server->server || stats == nullptr) {
+        return code(ts::Status::invalid_argument);
+    }
+    ts::cuda::ServeStats s;
+    const ts::Status st = server->server->run(
+        reinterpret_cast<const ts::cuda::ServeRequest *>(requests), count,
+        reinterpret_cast<ts::cuda::ServeOutcome *>(outcomes), s);
+    *stats = as<ts_serve_stats>(s);
+    return code(st);
+}
+
+extern "C" int ts_server_pool(const ts_server *server, ts_mutable_bytes *pool) {
+    if (server == nullptr || !server->server || pool == nullptr) {
+        return code(ts::Status::invalid_argument);
+    }
+    *pool = as<ts_mutable_bytes>(server->server->pool());
+    return 0;
+}
+
+extern "C" void ts_server_destroy(ts_server *server) {
+    delete server;
 }
 
 // Allocation-free one-image encode (declared in include/tilestream_c.h; no counterpart in the

@@ -5,7 +5,7 @@
 // What the plan builds is different: instead of DeviceImage/DeviceTile/DeviceSegment tables
 // split into 4096-tile windows with a binary search per block, every execution is one
 // persistent launch over a flat queue of self-contained tasks (tsk_decode_task, one per tile
-// to decode, 48 bytes), plus a 16-byte-aligned slot of row starts per predictive tile that the
+// to decode, 64 bytes), plus a 16-byte-aligned slot of row starts per predictive tile that the
 // kernel stages with the payload. The WorkspaceSpec reported to callers is still the
 // reference's per-window bound, so workspace_size() callers allocate what they always did.
 #include "plan.h"
@@ -305,6 +305,8 @@ Status draft_calibrate(const BatchRequest &request, Draft &d) {
     return Status::success;
 }
 
+} // namespace
+
 // Repeats the parser's structural checks that keep device reads inside the tile payload
 // (reference plan.cpp:237-279).
 Status check_tile(const ImageMetadata &m, std::uint64_t index) noexcept {
@@ -346,6 +348,8 @@ Status check_tile(const ImageMetadata &m, std::uint64_t index) noexcept {
     }
     return Status::success;
 }
+
+namespace {
 
 // The ROI clip of one tile: rows [row0, row1) and columns [col0, col1) of the tile, placed at
 // output (ox, oy); dst addresses tile column 0 of row row0 in the output. A tile whose rows are

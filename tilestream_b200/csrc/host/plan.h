@@ -91,6 +91,9 @@ struct PlanState {
     ~PlanState();
 };
 
+// The structural checks of tile `index` that keep device reads inside its payload.
+[[nodiscard]] Status check_tile(const ImageMetadata &m, std::uint64_t index) noexcept;
+
 [[nodiscard]] Status check_execution(const PlanState *plan, Operation operation,
                                      MutableBytes workspace, ResultBuffer results,
                                      cudaStream_t stream) noexcept;

@@ -497,42 +497,160 @@ __device__ __forceinline__ void fail(tsk_result *results, uint32_t image, uint32
     atomicCAS(&results[image].status, 0u, status);
 }
 
+// A 64-byte task record through the read-only path (records are never written during a launch).
+__device__ __forceinline__ tsk_decode_task load_task(const tsk_decode_task *p) {
+    union {
+        uint4 v[4];
+        tsk_decode_task t;
+    } u;
+    for (int k = 0; k < 4; ++k) {
+        u.v[k] = ld_nc_v4(reinterpret_cast<const uint4 *>(p) + k);
+    }
+    return u.t;
+}
+
+// Task sources of the persistent loop. The producer asks a source for the task at queue index
+// g = blockIdx.x + i * gridDim.x (increasing i); the consumers ask it for the calibration and
+// the bytes_written of a task's image.
+//
+// TableSource: a planned queue of tasks and its image table (every plan and mixed batch).
+struct TableSource {
+    static constexpr bool kTrusted = true;
+    const tsk_decode_task *tasks;
+    const tsk_decode_image *images;
+    uint32_t ntasks;
+
+    __device__ tsk_decode_task task(uint32_t g) {
+        return load_task(tasks + g);
+    }
+    __device__ uint32_t image_of(uint32_t g) const {
+        return tasks[g].image;
+    }
+    __device__ const tsk_decode_image &image(uint32_t i) const {
+        return images[i];
+    }
+    __device__ void calibration(const tsk_decode_task &t, StageHeader &h) const {
+        const tsk_decode_image &im = images[t.image];
+        const int64_t cx = static_cast<int64_t>(t.ox) - t.col0;
+        h.offset = im.offset;
+        h.gain = im.gain;
+        h.opitch = im.offset_pitch;
+        h.gpitch = im.gain_pitch;
+        h.omap = im.offset_map ? im.offset_map + t.oy * im.offset_pitch + cx * 4 : 0;
+        h.gmap = im.gain_map ? im.gain_map + t.oy * im.gain_pitch + cx * 4 : 0;
+    }
+    __device__ uint64_t result_bytes(const tsk_decode_task &t) const {
+        return images[t.image].result_bytes;
+    }
+};
+
+// ServeSource: a serving batch (the kernel's parameter block) over resident archives. Task g
+// is tile l = g - (first task of its request) of the request's ROI in row-major tile order;
+// its template is completed with the ROI clip that the host planner applies per task
+// (plan.cpp clip(), after reference plan.cpp:281-349), so no task table is uploaded.
+struct ServeSource {
+    static constexpr bool kTrusted = false;
+    const tsk_serve_batch *batch;
+    const tsk_serve_archive *archives;
+    uint32_t ntasks;
+    uint32_t cursor; // request of the last task asked for (indexes only increase)
+
+    __device__ tsk_decode_task task(uint32_t g) {
+        const tsk_serve_request *req = batch->requests;
+        while (g >= req[cursor].task_end) {
+            ++cursor; // g < ntasks == req[count - 1].task_end ends the walk
+        }
+        const tsk_serve_request &q = req[cursor];
+        const uint32_t l = g - (cursor != 0 ? req[cursor - 1].task_end : 0u);
+        const tsk_serve_archive &a = archives[q.archive];
+        const uint32_t trow = q.top + l / q.across;
+        const uint32_t tcol = q.left + l % q.across;
+        const tsk_decode_task *tpl = reinterpret_cast<const tsk_decode_task *>(a.tiles) +
+                                     static_cast<uint64_t>(trow) * a.tiles_across + tcol;
+        tsk_decode_task t = load_task(tpl);
+        t.image = cursor;
+        t.flags = static_cast<uint8_t>(t.flags | q.flags | (l == 0 ? TSK_FIRST : 0));
+        const uint64_t x = static_cast<uint64_t>(tcol) * a.tile_width;
+        const uint64_t y = static_cast<uint64_t>(trow) * a.tile_height;
+        const uint64_t rx1 = static_cast<uint64_t>(q.x) + q.width;
+        const uint64_t ry1 = static_cast<uint64_t>(q.y) + q.height;
+        t.row0 = static_cast<uint16_t>(q.y > y ? q.y - y : 0);
+        t.row1 = static_cast<uint16_t>(ry1 < y + t.height ? ry1 - y : t.height);
+        t.col0 = static_cast<uint16_t>(q.x > x ? q.x - x : 0);
+        t.col1 = static_cast<uint16_t>(rx1 < x + t.width ? rx1 - x : t.width);
+        t.ox = static_cast<uint32_t>(x + t.col0 - q.x);
+        t.oy = static_cast<uint32_t>(y + t.row0 - q.y);
+        const uint64_t esize = (t.flags & (TSK_F32 | TSK_CALIBRATED)) ? 4 : 2;
+        // Unsigned wrap-around gives the address before the region when t.ox < t.col0.
+        t.dst = q.out + t.oy * q.out_pitch + (static_cast<uint64_t>(t.ox) - t.col0) * esize;
+        t.pitch = q.out_pitch;
+        const bool class_width = t.width == 64 || t.width == 128 || t.width == 256;
+        if (class_width && t.col0 == 0 && t.col1 == t.width && ((t.dst | t.pitch) & 15u) == 0) {
+            t.flags |= TSK_FULL;
+        }
+        return t;
+    }
+    __device__ uint32_t image_of(uint32_t g) const {
+        uint32_t r = 0;
+        while (r + 1 < batch->count && g >= batch->requests[r].task_end) {
+            ++r;
+        }
+        return r;
+    }
+    __device__ const tsk_decode_image &image(uint32_t) const; // no trusted tasks
+    __device__ void calibration(const tsk_decode_task &t, StageHeader &h) const {
+        const tsk_serve_request &q = batch->requests[t.image];
+        h.offset = q.offset;
+        h.gain = q.gain;
+        h.opitch = h.gpitch = 0;
+        h.omap = h.gmap = 0;
+    }
+    __device__ uint64_t result_bytes(const tsk_decode_task &t) const {
+        const tsk_serve_request &q = batch->requests[t.image];
+        const uint64_t esize = (t.flags & (TSK_F32 | TSK_CALIBRATED)) ? 4 : 2;
+        return static_cast<uint64_t>(q.width) * q.height * esize;
+    }
+};
+
 // Producer: stages one task into stage s.
-template <typename Sh>
-__device__ void stage_task(Sh &sh, uint32_t s, const tsk_decode_task &t,
-                           const tsk_decode_image *images, const tsk_row_start *rowtab) {
+template <typename Sh, typename Source>
+__device__ void stage_task(Sh &sh, uint32_t s, const tsk_decode_task &t, const Source &source,
+                           const tsk_row_start *rowtab) {
     StageHeader &h = sh.header[s];
     uint64_t src = t.src;
     uint32_t words = static_cast<uint32_t>(t.words_or_tile);
     uint32_t mode = t.mode;
     uint32_t state = kStageOk;
-    if (t.flags & TSK_TRUSTED) {
-        const tsk_decode_image &im = images[t.image];
-        const volatile tsk_result *producer =
-            reinterpret_cast<const volatile tsk_result *>(im.encoder_result);
-        const uint32_t produced_status = producer->status;
-        const uint64_t produced_bytes = producer->bytes_written;
-        if (produced_status != 0) {
-            state = kStageSkip;
-        } else {
-            const uint64_t end = produced_bytes < im.capacity ? produced_bytes : im.capacity;
-            // The archive is only 4-byte aligned: read the entry as 32-bit words.
-            const uint32_t *e = reinterpret_cast<const uint32_t *>(t.src + 64 +
-                                                                   32 * t.words_or_tile);
-            const uint32_t e0 = e[0], e1 = e[1];
-            const uint64_t offset = e[2] | (static_cast<uint64_t>(e[3]) << 32);
-            const uint64_t length = e[4] | (static_cast<uint64_t>(e[5]) << 32);
-            const uint32_t ew = e1 & 0xffffu, eh = e1 >> 16;
-            const uint64_t s_bytes = (t.flags & TSK_F32) ? 4 : 2;
-            const uint64_t raw = (static_cast<uint64_t>(t.width) * t.height * s_bytes + 3) / 4 * 4;
-            mode = e0 & 0xffu;
-            if (mode > TSK_PREDICT || ew != t.width || eh != t.height || offset % 4 != 0 ||
-                length % 4 != 0 || length == 0 || length > raw || offset > end ||
-                length > end - offset) {
-                state = kStageMalformed;
+    if constexpr (Source::kTrusted) {
+        if (t.flags & TSK_TRUSTED) {
+            const tsk_decode_image &im = source.image(t.image);
+            const volatile tsk_result *producer =
+                reinterpret_cast<const volatile tsk_result *>(im.encoder_result);
+            const uint32_t produced_status = producer->status;
+            const uint64_t produced_bytes = producer->bytes_written;
+            if (produced_status != 0) {
+                state = kStageSkip;
             } else {
-                src = t.src + offset;
-                words = static_cast<uint32_t>(length / 4);
+                const uint64_t end = produced_bytes < im.capacity ? produced_bytes : im.capacity;
+                // The archive is only 4-byte aligned: read the entry as 32-bit words.
+                const uint32_t *e = reinterpret_cast<const uint32_t *>(t.src + 64 +
+                                                                       32 * t.words_or_tile);
+                const uint32_t e0 = e[0], e1 = e[1];
+                const uint64_t offset = e[2] | (static_cast<uint64_t>(e[3]) << 32);
+                const uint64_t length = e[4] | (static_cast<uint64_t>(e[5]) << 32);
+                const uint32_t ew = e1 & 0xffffu, eh = e1 >> 16;
+                const uint64_t s_bytes = (t.flags & TSK_F32) ? 4 : 2;
+                const uint64_t raw =
+                    (static_cast<uint64_t>(t.width) * t.height * s_bytes + 3) / 4 * 4;
+                mode = e0 & 0xffu;
+                if (mode > TSK_PREDICT || ew != t.width || eh != t.height || offset % 4 != 0 ||
+                    length % 4 != 0 || length == 0 || length > raw || offset > end ||
+                    length > end - offset) {
+                    state = kStageMalformed;
+                } else {
+                    src = t.src + offset;
+                    words = static_cast<uint32_t>(length / 4);
+                }
             }
         }
     }
@@ -571,14 +689,7 @@ __device__ void stage_task(Sh &sh, uint32_t s, const tsk_decode_task &t,
     }
     h.task = t;
     if (t.flags & TSK_CALIBRATED) {
-        const tsk_decode_image &im = images[t.image];
-        const int64_t cx = static_cast<int64_t>(t.ox) - t.col0;
-        h.offset = im.offset;
-        h.gain = im.gain;
-        h.opitch = im.offset_pitch;
-        h.gpitch = im.gain_pitch;
-        h.omap = im.offset_map ? im.offset_map + t.oy * im.offset_pitch + cx * 4 : 0;
-        h.gmap = im.gain_map ? im.gain_map + t.oy * im.gain_pitch + cx * 4 : 0;
+        source.calibration(t, h);
     }
     h.shift = shift;
     h.words = words;
@@ -587,14 +698,12 @@ __device__ void stage_task(Sh &sh, uint32_t s, const tsk_decode_task &t,
     mbar_arrive(&sh.full[s]);
 }
 
-// CW consumer warps, G16 columns per lane for uint16 rows; MinBlocks resident CTAs per SM.
+// The persistent loop over a task source: CW consumer warps, G16 columns per lane for uint16
+// rows.
 template <uint32_t MaxPayload, uint32_t Stages, uint32_t Paths, uint32_t CW, uint32_t G16,
-          uint32_t MinBlocks>
-__global__ void __launch_bounds__(threads_of(CW), MinBlocks)
-    decode_kernel(const tsk_decode_task *__restrict__ tasks, uint32_t ntasks,
-                  const tsk_decode_image *__restrict__ images,
-                  const tsk_row_start *__restrict__ rowtab, tsk_result *results, uint32_t one,
-                  uint32_t top) {
+          typename Source>
+__device__ __forceinline__ void decode_body(Source &source, const tsk_row_start *rowtab,
+                                            tsk_result *results, uint32_t one, uint32_t top) {
     using Sh = Shared<MaxPayload, Stages>;
     constexpr uint32_t kConsumers = CW * 32;
     extern __shared__ __align__(128) uint8_t smem_raw[];
@@ -608,6 +717,7 @@ __global__ void __launch_bounds__(threads_of(CW), MinBlocks)
         fence_barrier_init();
     }
     __syncthreads();
+    const uint32_t ntasks = source.ntasks;
     const uint32_t mine = blockIdx.x < ntasks ? (ntasks - 1 - blockIdx.x) / gridDim.x + 1 : 0;
 
     if (warp == CW) {
@@ -618,18 +728,18 @@ __global__ void __launch_bounds__(threads_of(CW), MinBlocks)
         }
         tsk_decode_task t{};
         if (mine != 0) {
-            t = tasks[blockIdx.x];
+            t = source.task(blockIdx.x);
         }
         for (uint32_t i = 0; i < mine; ++i) {
             const uint32_t s = i % Stages;
             tsk_decode_task next{};
             if (i + 1 < mine) {
-                next = tasks[blockIdx.x + (i + 1) * gridDim.x];
+                next = source.task(blockIdx.x + (i + 1) * gridDim.x);
             }
             if (i >= Stages && !mbar_wait(&sh.empty[s], ((i / Stages) - 1) & 1u)) {
                 return; // consumers stopped; they have reported the timeout
             }
-            stage_task(sh, s, t, images, rowtab);
+            stage_task(sh, s, t, source, rowtab);
             t = next;
         }
         return;
@@ -639,7 +749,7 @@ __global__ void __launch_bounds__(threads_of(CW), MinBlocks)
         const uint32_t s = i % Stages;
         if (!mbar_wait(&sh.full[s], (i / Stages) & 1u)) {
             if (threadIdx.x == 0) {
-                fail(results, tasks[blockIdx.x + i * gridDim.x].image, 9u); // cuda_error
+                fail(results, source.image_of(blockIdx.x + i * gridDim.x), 9u); // cuda_error
             }
             return;
         }
@@ -650,7 +760,6 @@ __global__ void __launch_bounds__(threads_of(CW), MinBlocks)
         const bool f32 = (t.flags & TSK_F32) != 0;
         const bool calibrated = (t.flags & TSK_CALIBRATED) != 0;
         const bool trusted = (t.flags & TSK_TRUSTED) != 0;
-        const tsk_decode_image *im = images + t.image;
         bool ok = state == kStageOk;
         if (trusted && ok && hmode == TSK_PREDICT) {
             if (threadIdx.x == 0) {
@@ -704,33 +813,64 @@ __global__ void __launch_bounds__(threads_of(CW), MinBlocks)
             mbar_arrive(&sh.empty[s]);
         }
         if (threadIdx.x == 0) {
-            if (trusted) {
-                if (state == kStageMalformed || (state == kStageOk && !ok)) {
-                    fail(results, t.image, 5u); // malformed_data
-                }
-                // Completion count: the last task of the image writes the final record.
-                __threadfence();
-                const uint32_t done = atomicAdd(&results[t.image].reserved, 1u);
-                if (done + 1 == im->tile_count) {
-                    __threadfence();
-                    uint32_t status =
-                        *reinterpret_cast<volatile uint32_t *>(&results[t.image].status);
-                    const uint32_t produced =
-                        reinterpret_cast<const volatile tsk_result *>(im->encoder_result)->status;
-                    if (produced != 0) {
-                        status = produced;
+            bool counted = false;
+            if constexpr (Source::kTrusted) {
+                if (trusted) {
+                    counted = true;
+                    const tsk_decode_image &im = source.image(t.image);
+                    if (state == kStageMalformed || (state == kStageOk && !ok)) {
+                        fail(results, t.image, 5u); // malformed_data
                     }
-                    results[t.image].reserved = 0;
-                    results[t.image].bytes_written = status == 0 ? im->result_bytes : 0;
-                    results[t.image].status = status;
+                    // Completion count: the last task of the image writes the final record.
+                    __threadfence();
+                    const uint32_t done = atomicAdd(&results[t.image].reserved, 1u);
+                    if (done + 1 == im.tile_count) {
+                        __threadfence();
+                        uint32_t status =
+                            *reinterpret_cast<volatile uint32_t *>(&results[t.image].status);
+                        const uint32_t produced =
+                            reinterpret_cast<const volatile tsk_result *>(im.encoder_result)
+                                ->status;
+                        if (produced != 0) {
+                            status = produced;
+                        }
+                        results[t.image].reserved = 0;
+                        results[t.image].bytes_written = status == 0 ? im.result_bytes : 0;
+                        results[t.image].status = status;
+                    }
                 }
-            } else if (t.flags & TSK_FIRST) {
+            }
+            if (!counted && (t.flags & TSK_FIRST)) {
                 results[t.image].status = 0;
                 results[t.image].reserved = 0;
-                results[t.image].bytes_written = im->result_bytes;
+                results[t.image].bytes_written = source.result_bytes(t);
             }
         }
     }
+}
+
+// A planned queue (every plan and mixed batch); MinBlocks resident CTAs per SM.
+template <uint32_t MaxPayload, uint32_t Stages, uint32_t Paths, uint32_t CW, uint32_t G16,
+          uint32_t MinBlocks>
+__global__ void __launch_bounds__(threads_of(CW), MinBlocks)
+    decode_kernel(const tsk_decode_task *__restrict__ tasks, uint32_t ntasks,
+                  const tsk_decode_image *__restrict__ images,
+                  const tsk_row_start *__restrict__ rowtab, tsk_result *results, uint32_t one,
+                  uint32_t top) {
+    TableSource source{tasks, images, ntasks};
+    decode_body<MaxPayload, Stages, Paths, CW, G16>(source, rowtab, results, one, top);
+}
+
+// A serving batch: the requests arrive in the parameter block.
+template <uint32_t MaxPayload, uint32_t Stages, uint32_t Paths, uint32_t CW, uint32_t G16,
+          uint32_t MinBlocks>
+__global__ void __launch_bounds__(threads_of(CW), MinBlocks)
+    serve_kernel(const __grid_constant__ tsk_serve_batch batch,
+                 const tsk_serve_archive *__restrict__ archives,
+                 const tsk_row_start *__restrict__ rowtab, tsk_result *results, uint32_t one,
+                 uint32_t top) {
+    ServeSource source{&batch, archives, batch.ntasks, 0};
+    decode_body<MaxPayload, Stages, Paths, CW, G16>(source, rowtab, results, one, top);
 }
 
 using KernelFn = void (*)(const tsk_decode_task *, uint32_t, const tsk_decode_image *,
@@ -788,6 +928,25 @@ Variant select(uint32_t paths, uint32_t shape) {
     }
     return narrow ? make<16384, 3, kU16 | kF32 | kPlain | kCal, 4, 16, 4>()
                   : make<16384, 3, kU16 | kF32 | kPlain | kCal>();
+}
+
+using ServeFn = void (*)(tsk_serve_batch, const tsk_serve_archive *, const tsk_row_start *,
+                         tsk_result *, uint32_t, uint32_t);
+
+struct ServeVariant {
+    ServeFn fn;
+    size_t smem;
+    uint32_t threads;
+};
+
+// Serving instances: uint16 archives (plain and scalar-calibrated requests), and any archives.
+ServeVariant select_serve(bool all_u16) {
+    if (all_u16) {
+        return {serve_kernel<8192, 4, kU16 | kPlain | kCal, 8, 8, 3>, sizeof(Shared<8192, 4>),
+                threads_of(8)};
+    }
+    return {serve_kernel<16384, 3, kU16 | kF32 | kPlain | kCal, 8, 8, 3>,
+            sizeof(Shared<16384, 3>), threads_of(8)};
 }
 
 } // namespace
@@ -870,4 +1029,29 @@ extern "C" int tsk_decode_graph(const tsk_decode_task *tasks, uint32_t ntasks,
     }
     *graph_out = graph;
     return cudaSuccess;
+}
+
+extern "C" int tsk_serve_prepare(int all_u16, int device, uint32_t *grid) {
+    const tsk::ServeVariant v = tsk::select_serve(all_u16 != 0);
+    cudaError_t e = cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(v.smem));
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v.fn, v.threads, v.smem);
+    if (e != cudaSuccess) return e;
+    int sms = 0;
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (e != cudaSuccess) return e;
+    *grid = static_cast<uint32_t>(sms) * static_cast<uint32_t>(per_sm < 1 ? 1 : per_sm);
+    return cudaSuccess;
+}
+
+extern "C" int tsk_serve_launch(const tsk_serve_batch *batch, const tsk_serve_archive *archives,
+                                const tsk_row_start *rows, tsk_result *results, uint32_t grid,
+                                int all_u16, cudaStream_t stream) {
+    if (batch->ntasks == 0) return cudaSuccess;
+    const tsk::ServeVariant v = tsk::select_serve(all_u16 != 0);
+    const uint32_t blocks = grid < batch->ntasks ? grid : batch->ntasks;
+    v.fn<<<blocks, v.threads, v.smem, stream>>>(*batch, archives, rows, results, 1u, 0x80000000u);
+    return cudaGetLastError();
 }

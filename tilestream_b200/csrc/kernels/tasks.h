@@ -137,6 +137,40 @@ typedef struct __align__(16) {
     uint32_t reserved[3];
 } tsk_calib_image;
 
+// --- serving: resident archives, requests expanded into tile tasks on the device -------------
+
+// One resident archive. Its tile templates are decode tasks with the archive-dependent fields
+// set (src, words_or_tile, width, height, mode, rows_at, TSK_F32); a request fills in the rest.
+typedef struct __align__(16) {
+    uint64_t tiles;        // device address of tsk_decode_task[tiles_across * tiles_down]
+    uint32_t tiles_across;
+    uint16_t tile_width, tile_height;
+    uint32_t type; // 1 = uint16, 2 = float32
+    uint32_t reserved;
+} tsk_serve_archive;
+
+// One request: an ROI of one archive, written packed at out with out_pitch. 64 bytes.
+typedef struct __align__(16) {
+    uint64_t out;
+    uint64_t out_pitch;
+    uint32_t task_end; // tasks of the batch up to and including this request
+    uint32_t archive;
+    uint32_t x, y, width, height; // ROI in archive pixels
+    uint32_t left, top, across;   // first tile column and row of the ROI; tiles per ROI row
+    uint32_t flags;               // TSK_CALIBRATED or 0
+    float offset, gain;           // scalar calibration
+} tsk_serve_request;
+
+// A batch of requests, passed to the kernel as its parameter block (no upload): the whole
+// launch's parameters stay below the classic 4 KB limit.
+#define TSK_SERVE_MAX_BATCH 48
+typedef struct __align__(16) {
+    uint32_t count;
+    uint32_t ntasks; // requests[count - 1].task_end
+    uint32_t reserved[2];
+    tsk_serve_request requests[TSK_SERVE_MAX_BATCH];
+} tsk_serve_batch;
+
 // DeviceResult as seen by the kernels (types.h: {status, reserved, bytes_written}).
 typedef struct {
     uint32_t status;
@@ -159,6 +193,15 @@ int tsk_decode_graph(const tsk_decode_task *tasks, uint32_t ntasks,
                      const tsk_decode_image *images, const tsk_row_start *rows,
                      tsk_result *results, uint32_t result_count, int clear_results,
                      tsk_decode_config config, cudaGraph_t *graph, cudaGraphExec_t *exec);
+
+// Decodes one serving batch: tile tasks are derived from the requests and the resident archive
+// templates inside the kernel. results: one record per request of the batch. all_u16: every
+// archive holds uint16 samples (selects the smaller-stage kernel instance).
+int tsk_serve_launch(const tsk_serve_batch *batch, const tsk_serve_archive *archives,
+                     const tsk_row_start *rows, tsk_result *results, uint32_t grid, int all_u16,
+                     cudaStream_t stream);
+// Loads the serving kernel instance and returns its persistent grid (SMs x resident CTAs).
+int tsk_serve_prepare(int all_u16, int device, uint32_t *grid);
 
 // Encodes every tile of every image in one pass. state: 8 * (total_tiles + 2) bytes of
 // workspace, cleared by the launcher in stream order.

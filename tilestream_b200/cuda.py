@@ -160,3 +160,76 @@ def prepare_mixed_batch(items, results, stream=None, graph=True, autotune=False,
     if st == 0:
         return Status.success, MixedBatch(h.value)
     return Status(st), None
+
+
+class Server:
+    """An owned tilestream::cuda::Server: archives resident in device memory, ROI and
+    calibrated-ROI requests admitted by output-pool memory and batched into the persistent
+    decoder, several batches in flight (continuous batching).
+
+    Archives are added with their device bytes and parsed metadata (both kept alive here),
+    then sealed; run() serves a request stream and returns (Status, outcomes, stats)."""
+
+    def __init__(self, pool_bytes=1 << 30, max_batch=48, max_inflight=4, max_batch_tiles=1 << 22,
+                 retain_outputs=False, serial=False):
+        self.options = N.ServeOptions(pool_bytes, max_batch, max_inflight, max_batch_tiles,
+                                      1 if retain_outputs else 0, 1 if serial else 0)
+        h = C.c_void_p(0)
+        st = N.lib().ts_server_create(C.byref(self.options), C.byref(h))
+        if st != 0:
+            raise RuntimeError(f"ts_server_create: {Status(st).name}")
+        self.handle = h.value
+        self._keep = []
+
+    def add_archive(self, device_bytes, metadata, owner=None) -> tuple[Status, int]:
+        """device_bytes: ConstBytes of the archive in device memory; metadata: a parsed
+        ImageMetadata (api.parse_metadata); owner: the object holding the device memory (kept
+        alive with the server)."""
+        i = C.c_uint32(0)
+        st = N.lib().ts_server_add_archive(self.handle, device_bytes, metadata.handle,
+                                           C.byref(i))
+        if st == 0:
+            self._keep.append((owner, metadata))
+        return Status(st), i.value
+
+    def seal(self) -> Status:
+        return Status(N.lib().ts_server_seal(self.handle))
+
+    def pool(self) -> N.MutableBytes:
+        p = N.MutableBytes()
+        N.lib().ts_server_pool(self.handle, C.byref(p))
+        return p
+
+    def run(self, requests):
+        """requests: a sequence of N.ServeRequest or a ctypes array of them."""
+        if isinstance(requests, C.Array):
+            arr, count = requests, len(requests)
+        else:
+            requests = list(requests)
+            arr = (N.ServeRequest * max(1, len(requests)))(*requests)
+            count = len(requests)
+        outcomes = (N.ServeOutcome * max(1, count))()
+        stats = N.ServeStats()
+        st = N.lib().ts_server_run(self.handle, arr, count, outcomes, C.byref(stats))
+        return Status(st), outcomes, stats
+
+    def __del__(self):
+        if getattr(self, "handle", None):
+            N.lib().ts_server_destroy(self.handle)
+            self.handle = None
+
+
+def serve_requests(stream: dict, scale_arrivals: float = 1.0):
+    """A ctypes array of ServeRequest from the arrays of workloads.serving_requests."""
+    n = len(stream["arrival_us"])
+    arr = (N.ServeRequest * max(1, n))()
+    for i in range(n):
+        r = arr[i]
+        r.archive = int(stream["archive"][i])
+        r.roi = N.Roi(int(stream["x"][i]), int(stream["y"][i]), int(stream["width"][i]),
+                      int(stream["height"][i]))
+        r.calibrated = 1 if stream["calibrated"][i] else 0
+        r.offset = float(stream["offset"][i])
+        r.gain = float(stream["gain"][i])
+        r.arrival_us = float(stream["arrival_us"][i]) * scale_arrivals
+    return arr if n else (N.ServeRequest * 0)()

@@ -10,6 +10,9 @@ pixels:
   mantissa bits random, 0.1 % special words (+-0, +-inf, NaN with random payloads, subnormals)
   (configs 3 and 4).
 * `calibration_maps` offset ~ N(100, 5), gain ~ U(0.9, 1.1) FP32 maps (config 3).
+* `serving_requests` a request stream: Poisson arrivals, ROI sides log-uniform in [32, 4096]
+  at a uniform offset inside the archive, 40 % with scalar calibration (offset 100.0, gain
+  1.05) (config 5).
 
 RNG: numpy PCG64 seeded with the frame seed; sin/cos come from the C library through `math` on
 1-D axes, so results do not depend on numpy's SIMD transcendental kernels. The `*_torch`
@@ -136,3 +139,34 @@ def field_frame_torch(width: int, height: int, seed: int, device="cuda"):
         table = torch.where(kind == 4, sign | 0x7F800000 | mant, table)
         words[special] = table
     return words
+
+
+def serving_requests(count: int, archives: int, width: int, height: int, rate_per_s: float,
+                     seed: int, min_side: int = 32, max_side: int = 4096,
+                     calibrated_fraction: float = 0.4, offset: float = 100.0,
+                     gain: float = 1.05) -> dict:
+    """A seeded request stream over `archives` archives of width x height pixels.
+
+    Arrivals are a Poisson process of the given rate (exponential gaps, first request at the
+    first gap). Each side is exp(U(ln min_side, ln max_side)) rounded, capped at the archive's
+    size; the offset is uniform over the positions that keep the ROI inside the archive.
+    Returns numpy arrays: arrival_us, archive, x, y, width, height, calibrated, offset, gain."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    gaps = rng.exponential(1e6 / rate_per_s, count)
+    arrival = np.cumsum(gaps)
+    lo = math.log(min_side)
+
+    def sides(limit):
+        hi = math.log(max(min(max_side, limit), min_side))
+        v = np.rint(np.exp(rng.uniform(lo, hi, count))).astype(np.int64)
+        return np.clip(v, min(min_side, limit), min(max_side, limit))
+
+    w = sides(width)
+    h = sides(height)
+    x = (rng.random(count) * (width - w + 1)).astype(np.int64)
+    y = (rng.random(count) * (height - h + 1)).astype(np.int64)
+    archive = rng.integers(0, archives, count)
+    calibrated = rng.random(count) < calibrated_fraction
+    return {"arrival_us": arrival, "archive": archive, "x": x, "y": y, "width": w, "height": h,
+            "calibrated": calibrated, "offset": np.full(count, offset, np.float32),
+            "gain": np.full(count, gain, np.float32)}
