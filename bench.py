@@ -192,6 +192,22 @@ def prepare_workload(torch, stream, copies: int):
     return frame, shapes, workspace, results
 
 
+def max_over_ranks(value: float, world: int, dist, device: str) -> float:
+    """The largest value over the ranks (every rank gets it): the timed region of a multi-GPU
+    run lasts as long as its slowest rank."""
+    if world == 1:
+        return value
+    import torch
+    t = torch.tensor([value], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_gbs(bytes_per_step_per_rank: int, steps: int, world: int, ms: float) -> float:
+    """Whole-job GB/s: every rank decodes bytes_per_step_per_rank per step (weak scaling)."""
+    return bytes_per_step_per_rank * steps * world / (ms / 1e3) / 1e9
+
+
 def run_ours(args, rank, world, device, torch, dist):
     from tilestream_b200 import api, cuda
     from tilestream_b200.api import Status
@@ -255,14 +271,10 @@ def run_ours(args, rank, world, device, torch, dist):
         torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    ms = start.elapsed_time(end)
-    if world > 1:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(start.elapsed_time(end), world, dist, "cuda")
     step_ms = ms / args.steps
     decoded_per_step = 3 * W * H * 2
-    value = decoded_per_step * args.steps * world / (ms / 1e3) / 1e9
+    value = aggregate_gbs(decoded_per_step, args.steps, world, ms)
 
     # Per-shape device time (outside the timed region, same method).
     per_shape = {}
