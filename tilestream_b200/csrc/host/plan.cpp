@@ -664,7 +664,8 @@ bool upload(void *storage, std::uint64_t at, const std::vector<T> &v, cudaStream
 std::uint32_t decode_shape() {
     static const std::uint32_t shape = [] {
         const char *env = std::getenv("TILESTREAM_DECODE_SHAPE");
-        return env != nullptr ? static_cast<std::uint32_t>(std::strtoul(env, nullptr, 10)) % 4
+        return env != nullptr ? static_cast<std::uint32_t>(std::strtoul(env, nullptr, 10)) %
+                                    TSK_DECODE_SHAPES
                               : 2u;
     }();
     return shape;
@@ -1054,9 +1055,10 @@ Status autotune(detail::PlanState &p, tsk_result *results, const char *cache, cu
         return detail::cuda_status(apply(hit->second.shape, hit->second.per_sm), "tuned config");
     }
     const bool plain_u16 = p.config.paths == (TSK_PATH_U16 | TSK_PATH_PLAIN);
-    const std::uint32_t shapes_all[] = {0, 1, 2, 3}, shapes_two[] = {0, 2};
+    const std::uint32_t shapes_all[TSK_DECODE_SHAPES] = {0, 1, 2, 3, 4, 5},
+                        shapes_two[] = {0, 2};
     const std::uint32_t *shapes = plain_u16 ? shapes_all : shapes_two;
-    const std::size_t nshapes = plain_u16 ? 4 : 2;
+    const std::size_t nshapes = plain_u16 ? TSK_DECODE_SHAPES : 2;
     cudaEvent_t start = nullptr, stop = nullptr;
     if (cudaEventCreate(&start) != cudaSuccess || cudaEventCreate(&stop) != cudaSuccess) {
         return detail::cuda_failure("cudaEventCreate");

@@ -111,7 +111,8 @@ struct Ctx {
 // Pipe balance. On this SM the integer ALU pipe (logic, shifts, adds) and the FMA pipe
 // (integer multiply-add) each run at half the issue rate, and the uint16 decode is ALU-bound.
 // Additions written as multiply-adds by a runtime 1 (a kernel argument the compiler cannot
-// fold) execute on the FMA pipe instead; so does the left shift by 31 of the sign extraction.
+// fold) execute on the FMA pipe instead, and so do the inverse zigzag's shifts, written as
+// multiplies by runtime powers of two (unzig16).
 struct Pipes {
     uint32_t one; // 1
     uint32_t top; // 0x80000000
@@ -123,12 +124,17 @@ __device__ __forceinline__ uint32_t fma_add(uint32_t a, uint32_t b, const Pipes 
     return d;
 }
 
-// All ones when bit 0 of z is set, else zero: (z << 31) >> 31 (arithmetic), the shift as an
-// FMA-pipe multiply.
-__device__ __forceinline__ uint32_t low_bit_mask(uint32_t z, const Pipes &p) {
-    uint32_t d;
-    asm("mul.lo.u32 %0, %1, %2;" : "=r"(d) : "r"(z), "r"(p.top));
-    return static_cast<uint32_t>(static_cast<int32_t>(d) >> 31);
+// Inverse zigzag of the item whose lowest bit is bit `at` of w, from the multiplier
+// m = 2^(31 - at) (0 for an empty row): the magnitude (w >> (at + 1)) & mh and the sign bit
+// moved to bit 31 are products on the FMA pipe (the multipliers are runtime values, so the
+// compiler keeps them as multiplies); the sign mask is an arithmetic shift and the combination
+// one logic op, both on the ALU pipe. Exact in the low 16 bits, which is all a uint16 sum uses.
+__device__ __forceinline__ uint32_t unzig16(uint32_t w, uint32_t m, uint32_t mh) {
+    uint32_t h, lo;
+    asm("mul.hi.u32 %0, %1, %2;" : "=r"(h) : "r"(w), "r"(m));
+    asm("mul.lo.u32 %0, %1, %2;" : "=r"(lo) : "r"(w), "r"(m));
+    const uint32_t sign = static_cast<uint32_t>(static_cast<int32_t>(lo) >> 31);
+    return (h & mh) ^ sign;
 }
 
 // uint16 rows (b <= 16): the 64-bit window of the packed words that starts at the bit of item
@@ -181,15 +187,11 @@ template <uint32_t G, bool F32, bool Partial>
 __device__ __forceinline__ void terms(const uint32_t *packed, uint32_t c0, uint32_t w, uint32_t b,
                                       const Pipes &pipes, uint32_t (&t)[G]) {
     if constexpr (!F32) {
-        // uint16, b <= 16: four residuals per 64-bit window.
-        if (b == 0) {
-#pragma unroll
-            for (uint32_t k = 0; k < G; ++k) {
-                t[k] = 0;
-            }
-            return;
-        }
-        const uint32_t mh = low_mask(b) >> 1; // the magnitude bits of a zigzag value
+        // uint16, b <= 16: four residuals per 64-bit window. An empty row (b = 0) has no packed
+        // words: its multipliers are zero, so every term is zero whatever the window holds.
+        const uint32_t mh = low_mask(b) >> 1;           // the magnitude bits of a zigzag value
+        const uint32_t m0 = b != 0 ? pipes.top : 0u;    // 2^31: the item at bit 0
+        const uint32_t m1 = b != 0 ? pipes.top >> b : 0u; // 2^(31 - b): the item at bit b
 #pragma unroll
         for (uint32_t q = 0; q < G; q += 4) {
             uint32_t x0, x1;
@@ -200,18 +202,13 @@ __device__ __forceinline__ void terms(const uint32_t *packed, uint32_t c0, uint3
                     keep_bits(x0, x1, items * b);
                 }
             }
-            uint32_t z[4];
-            z[0] = x0;
-            z[1] = __funnelshift_rc(x0, x1, b);
+            // Items q, q + 1 lie in x0 (2b <= 32 bits) and items q + 2, q + 3 in the word that
+            // starts 2b bits later. Inverse zigzag as an unsigned delta: z/2 or -(z/2) - 1.
             const uint32_t y0 = __funnelshift_rc(x0, x1, 2 * b);
-            const uint32_t y1 = __funnelshift_rc(x1, 0u, 2 * b);
-            z[2] = y0;
-            z[3] = __funnelshift_rc(y0, y1, b);
-#pragma unroll
-            for (uint32_t k = 0; k < 4; ++k) {
-                // Inverse zigzag as an unsigned delta: z/2 or -(z/2) - 1, modulo 2^32.
-                t[q + k] = ((z[k] >> 1) & mh) ^ low_bit_mask(z[k], pipes);
-            }
+            t[q] = unzig16(x0, m0, mh);
+            t[q + 1] = unzig16(x0, m1, mh);
+            t[q + 2] = unzig16(y0, m0, mh);
+            t[q + 3] = unzig16(y0, m1, mh);
         }
     } else {
         // FP32 words, b <= 32: two residuals per 64-bit window.
@@ -388,11 +385,16 @@ __device__ void decode_rows(const Ctx &x, const uint32_t *payload, const uint16_
                         t[k] = 0;
                     }
                 }
+                // Two independent running sums over the halves of the group (half the
+                // dependency chain), joined when the outputs are formed.
+                constexpr uint32_t H = G / 2;
 #pragma unroll
                 for (uint32_t k = 1; k < G; ++k) {
-                    t[k] = add(t[k - 1], t[k]);
+                    if (k != H) {
+                        t[k] = add(t[k - 1], t[k]);
+                    }
                 }
-                const uint32_t total = t[G - 1];
+                const uint32_t total = add(t[H - 1], t[G - 1]);
                 uint32_t inclusive = total;
 #pragma unroll
                 for (uint32_t d = 1; d < LW; d <<= 1) {
@@ -404,10 +406,11 @@ __device__ void decode_rows(const Ctx &x, const uint32_t *payload, const uint16_
                 const uint32_t before = add(carry, uncombine<F32>(inclusive, total));
                 carry = add(carry, __shfl_sync(kFull, inclusive, LW - 1, LW));
                 if (live) {
+                    const uint32_t mid = add(before, t[H - 1]);
                     uint32_t v[G];
 #pragma unroll
                     for (uint32_t k = 0; k < G; ++k) {
-                        v[k] = add(before, t[k]);
+                        v[k] = add(k < H ? before : mid, t[k]);
                     }
                     store<G, F32, Cal, Full>(x, line, orow, grow, c0, v);
                 }
@@ -893,12 +896,13 @@ Variant make() {
             sizeof(Shared<MaxPayload, Stages>), threads_of(CW)};
 }
 
-// Shapes: 0 = 8 consumer warps x 8 uint16 columns per lane, 1 = 8 x 16, 2 = 4 x 16, 3 = 4 x 8.
-// The plain uint16 instance has all four; the others have shapes 0 and 2 (odd shapes map to
-// those).
+// Shapes of the plain uint16 instance (consumer warps x uint16 columns per lane, stages,
+// resident CTAs per SM): 0 = 8 x 8, 4 stages, 4; 1 = 8 x 16, 4, 3; 2 = 4 x 16, 4, 5;
+// 3 = 4 x 8, 4, 6; 4 = 4 x 16, 4, 6 (64 registers); 5 = 4 x 16, 3, 7 (56 registers). The other
+// instances have shapes 0 and 2 (odd shapes map to 0, even ones to 2).
 Variant select(uint32_t paths, uint32_t shape) {
     const bool f32 = paths & kF32, u16 = paths & kU16, plain = paths & kPlain, c = paths & kCal;
-    const bool narrow = shape == 2 || shape == 3; // four consumer warps
+    const bool narrow = shape % 2 == 0 && shape != 0; // four consumer warps
     if (!f32) {
         if (plain && !c) {
             switch (shape) {
@@ -908,6 +912,10 @@ Variant select(uint32_t paths, uint32_t shape) {
                 return make<8192, 4, kU16 | kPlain, 4, 16, 5>();
             case 3:
                 return make<8192, 4, kU16 | kPlain, 4, 8, 6>();
+            case 4:
+                return make<8192, 4, kU16 | kPlain, 4, 16, 6>();
+            case 5:
+                return make<8192, 3, kU16 | kPlain, 4, 16, 7>();
             default:
                 return make<8192, 4, kU16 | kPlain, 8, 8, 4>();
             }

@@ -34,21 +34,25 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
                  : "memory");
 }
 
-// One bounded probe of the phase with the given parity; true once it has completed.
+// One bounded probe of the phase with the given parity; true once it has completed. The
+// thread may be suspended until the phase completes, for at most about kSuspendNs, so a waiting
+// warp issues few instructions.
+constexpr uint32_t kSuspendNs = 2000;
 __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
     uint32_t done;
     asm volatile("{\n\t.reg .pred p;\n\t"
-                 "mbarrier.try_wait.parity.acquire.cta.shared::cta.b64 p, [%1], %2;\n\t"
+                 "mbarrier.try_wait.parity.acquire.cta.shared::cta.b64 p, [%1], %2, %3;\n\t"
                  "selp.u32 %0, 1, 0, p;\n\t}"
                  : "=r"(done)
-                 : "r"(smem_addr(bar)), "r"(parity)
+                 : "r"(smem_addr(bar)), "r"(parity), "n"(kSuspendNs)
                  : "memory");
     return done != 0;
 }
 
-// Waits with an iteration limit; false when the limit was reached (the caller reports it).
+// Waits with an iteration limit (at most about 2^21 x 2 us); false when the limit was reached
+// (the caller reports it).
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
-    constexpr uint32_t kLimit = 1u << 24;
+    constexpr uint32_t kLimit = 1u << 21;
     for (uint32_t i = 0; i < kLimit; ++i) {
         if (mbar_try_wait(bar, parity)) {
             return true;

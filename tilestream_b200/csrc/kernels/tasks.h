@@ -96,8 +96,13 @@ typedef struct {
     uint32_t per_sm; // resident CTAs per SM at the kernel's occupancy
     uint32_t smem;   // dynamic shared memory per CTA in bytes
     uint32_t paths;  // TSK_PATH_* mask selecting the kernel instance
-    uint32_t shape;  // plain uint16 kernel shape (consumer warps x columns per lane), 0-3
+    uint32_t shape;  // plain uint16 kernel shape, 0 .. TSK_DECODE_SHAPES - 1 (decode.cu)
 } tsk_decode_config;
+
+// Kernel shapes of the plain uint16 decoder (consumer warps, columns per lane, stages and
+// resident CTAs per SM; listed in decode.cu). Other instances map odd shapes to 0 and even
+// shapes to 2.
+#define TSK_DECODE_SHAPES 6
 
 // One image to encode. 96 bytes.
 typedef struct __align__(16) {
