@@ -720,12 +720,18 @@ __device__ __forceinline__ void decode_body(Source &source, const tsk_row_start 
         fence_barrier_init();
     }
     __syncthreads();
+    if (threadIdx.x == 0) {
+        griddep_launch_dependents();
+    }
     const uint32_t ntasks = source.ntasks;
     const uint32_t mine = blockIdx.x < ntasks ? (ntasks - 1 - blockIdx.x) / gridDim.x + 1 : 0;
 
     if (warp == CW) {
         // Producer warp: lane 0 issues everything. The next task record is loaded before
-        // waiting for a free stage, so its latency overlaps the consumers' work.
+        // waiting for a free stage, so its latency overlaps the consumers' work. Task records
+        // are the plan's (or the server's) own tables, written before any launch, so the first
+        // one is read before waiting for the stream's previous grid; payloads, which that grid
+        // may have produced, are read after.
         if (lane != 0) {
             return;
         }
@@ -733,6 +739,7 @@ __device__ __forceinline__ void decode_body(Source &source, const tsk_row_start 
         if (mine != 0) {
             t = source.task(blockIdx.x);
         }
+        griddep_wait();
         for (uint32_t i = 0; i < mine; ++i) {
             const uint32_t s = i % Stages;
             tsk_decode_task next{};
@@ -748,6 +755,9 @@ __device__ __forceinline__ void decode_body(Source &source, const tsk_row_start 
         return;
     }
 
+    // Consumers write outputs and result records, which the stream's previous grid may still
+    // be reading or writing.
+    griddep_wait();
     for (uint32_t i = 0; i < mine; ++i) {
         const uint32_t s = i % Stages;
         if (!mbar_wait(&sh.full[s], (i / Stages) & 1u)) {
@@ -983,15 +993,26 @@ extern "C" int tsk_decode_prepare(tsk_decode_config *config, uint32_t ntasks, in
     return cudaSuccess;
 }
 
+// Launched as a programmatic dependent of the stream's previous grid: this grid's CTAs may
+// start (barrier set-up, first task record) while that grid finishes, and wait for it before
+// touching payloads, outputs or results (griddep_wait in decode_body).
 extern "C" int tsk_decode_launch(const tsk_decode_task *tasks, uint32_t ntasks,
                                  const tsk_decode_image *images, const tsk_row_start *rows,
                                  tsk_result *results, tsk_decode_config config,
                                  cudaStream_t stream) {
     if (ntasks == 0) return cudaSuccess;
     const tsk::Variant v = tsk::select(config.paths, config.shape);
-    v.fn<<<config.grid, v.threads, v.smem, stream>>>(tasks, ntasks, images, rows, results, 1u,
-                                                     0x80000000u);
-    return cudaGetLastError();
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(config.grid);
+    cfg.blockDim = dim3(v.threads);
+    cfg.dynamicSmemBytes = v.smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, v.fn, tasks, ntasks, images, rows, results, 1u, 0x80000000u);
 }
 
 // A CUDA graph of one execution: a clear of the result records when the plan has trusted images

@@ -84,6 +84,17 @@ __device__ __forceinline__ void cp_async_arrive(uint64_t *bar) {
                  : "memory");
 }
 
+// Programmatic dependent launch. wait: blocks until the grids this one depends on in its
+// stream have completed and their memory is visible (immediately when the launch had no
+// programmatic dependency). launch_dependents: lets the next grid of the stream start its
+// prologue once every CTA of this grid has issued it or exited.
+__device__ __forceinline__ void griddep_wait() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+__device__ __forceinline__ void griddep_launch_dependents() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // Named barrier over a subset of the CTA's warps.
 __device__ __forceinline__ void named_sync(uint32_t id, uint32_t threads) {
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(threads) : "memory");
