@@ -1055,7 +1055,7 @@ Status autotune(detail::PlanState &p, tsk_result *results, const char *cache, cu
         return detail::cuda_status(apply(hit->second.shape, hit->second.per_sm), "tuned config");
     }
     const bool plain_u16 = p.config.paths == (TSK_PATH_U16 | TSK_PATH_PLAIN);
-    const std::uint32_t shapes_all[TSK_DECODE_SHAPES] = {0, 1, 2, 3, 4, 5},
+    const std::uint32_t shapes_all[TSK_DECODE_SHAPES] = {0, 1, 2, 3, 4, 5, 6, 7},
                         shapes_two[] = {0, 2};
     const std::uint32_t *shapes = plain_u16 ? shapes_all : shapes_two;
     const std::size_t nshapes = plain_u16 ? TSK_DECODE_SHAPES : 2;

@@ -908,8 +908,9 @@ Variant make() {
 
 // Shapes of the plain uint16 instance (consumer warps x uint16 columns per lane, stages,
 // resident CTAs per SM): 0 = 8 x 8, 4 stages, 4; 1 = 8 x 16, 4, 3; 2 = 4 x 16, 4, 5;
-// 3 = 4 x 8, 4, 6; 4 = 4 x 16, 4, 6 (64 registers); 5 = 4 x 16, 3, 7 (56 registers). The other
-// instances have shapes 0 and 2 (odd shapes map to 0, even ones to 2).
+// 3 = 4 x 8, 4, 6; 4 = 4 x 16, 4, 6 (64 registers); 5 = 4 x 16, 3, 7 (56 registers);
+// 6 = 4 x 32, 4, 3; 7 = 4 x 32, 4, 4. The other instances have shapes 0 and 2 (odd shapes map
+// to 0, even ones to 2).
 Variant select(uint32_t paths, uint32_t shape) {
     const bool f32 = paths & kF32, u16 = paths & kU16, plain = paths & kPlain, c = paths & kCal;
     const bool narrow = shape % 2 == 0 && shape != 0; // four consumer warps
@@ -926,6 +927,10 @@ Variant select(uint32_t paths, uint32_t shape) {
                 return make<8192, 4, kU16 | kPlain, 4, 16, 6>();
             case 5:
                 return make<8192, 3, kU16 | kPlain, 4, 16, 7>();
+            case 6:
+                return make<8192, 4, kU16 | kPlain, 4, 32, 3>();
+            case 7:
+                return make<8192, 4, kU16 | kPlain, 4, 32, 4>();
             default:
                 return make<8192, 4, kU16 | kPlain, 8, 8, 4>();
             }
