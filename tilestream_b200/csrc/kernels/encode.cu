@@ -1,23 +1,27 @@
-// Single-pass canonical .tsc encoder for sm_100a.
+// Single-launch canonical .tsc encoder for sm_100a.
 //
 // The reference encodes a window with four launches and a library scan: analyze (residuals to
 // a 16 KiB-per-tile global workspace), cub::DeviceScan over tile lengths, pack (re-reading the
 // input and the residuals) and finish (src/cuda/encoder.cu:62-327). Here one persistent kernel
-// does all of it and reads each input pixel once:
+// does all of it:
 //
-//  1. a CTA takes the next tile in batch order from an atomic counter, loads its pixels into
-//     shared memory and computes the residuals (zigzag mod 2^16 or XOR, encoder.cpp:32-37);
-//  2. one warp per row OR-reduces the residuals with shuffles; the row width is the index of
-//     the highest set bit (docs/format.md:101), the row costs are scanned with a warp shuffle
-//     scan, and the canonical mode is chosen with the tie order RAW < CONSTANT < PREDICT
+//  1. a CTA claims the next chunk of k consecutive tiles (in batch order, from an atomic
+//     counter; k = ceil(tiles / grid), at most kMaxChunk) and, tile by tile, loads the pixels
+//     into shared memory and computes the residuals (zigzag mod 2^16 or XOR, encoder.cpp:32-37);
+//     one warp per row OR-reduces them with shuffles, the row width is the index of the highest
+//     set bit (docs/format.md:101), the row costs are scanned with a warp shuffle scan, and the
+//     canonical mode is chosen with the tie order RAW < CONSTANT < PREDICT
 //     (docs/format.md:103-109, encoder.cpp:69-78);
-//  3. the tile's payload offset is the exclusive prefix of the lengths of the earlier tiles of
-//     the same image, found by a decoupled look-back over per-tile flags in the workspace
-//     (tile i publishes its length at once and its inclusive prefix when known; waits are
-//     bounded and report cuda_error instead of hanging);
-//  4. the index entry and every payload word are written by exactly one thread, gathering the
-//     residuals that overlap the word (encoder.cu:157-173 does the same from global memory);
-//  5. the last tile of an image writes the 64-byte header and the image's DeviceResult.
+//  2. the chunk publishes the summed lengths of its tiles of its last image; one warp then looks
+//     back over the earlier chunks of its first image, 32 chunks per step, stopping at the
+//     image's first chunk or at a chunk that has published its inclusive prefix. Every chunk
+//     publishes its sum as soon as its own tiles are analysed, so the look-back waits for no
+//     chain of prefixes (a look-back per tile would: tiles are small and many are in flight).
+//     Waits are bounded and report cuda_error instead of hanging;
+//  3. the CTA reloads each tile of the chunk (still in L2), recomputes its residuals and writes
+//     the index entry and every payload word, each word by exactly one thread (encoder.cu:157-173
+//     gathers the same bits from global memory);
+//  4. the last tile of an image writes the 64-byte header and the image's DeviceResult.
 #include "ptx.cuh"
 #include "tasks.h"
 
@@ -28,30 +32,40 @@ namespace tsk {
 namespace {
 
 constexpr uint32_t kThreads = 256;
-constexpr uint32_t kWarps = kThreads / 32;
 constexpr uint64_t kAggregate = 1ull << 62;
 constexpr uint64_t kPrefix = 2ull << 62;
 constexpr uint64_t kValue = (1ull << 62) - 1;
 
+constexpr uint32_t kMaxChunk = 8;
+
 struct EncodeShared {
-    uint32_t px[TSK_TILE_PIXELS];
-    uint32_t res[TSK_TILE_PIXELS]; // res[r * w + c] = residual of column c (c >= 1)
+    // Two tile buffers: the tile being analysed and the next one in flight. Rows are packed
+    // (w samples each), as uint16 or FP32 words.
+    alignas(16) uint32_t raw[2][TSK_TILE_PIXELS];
+    uint32_t stage[TSK_PAYLOAD_BYTES / 4]; // the tile payload being written (PREDICT)
+    uint32_t row_or[TSK_MAX_ROWS];         // OR of each row's residuals
     uint32_t bits[TSK_MAX_ROWS];
     uint32_t row_word[TSK_MAX_ROWS + 1]; // first payload word of each row
-    uint64_t offset;                     // absolute file offset of the payload
-    uint64_t inclusive;                  // prefix including this tile
-    uint64_t tile_id;
     uint32_t mode;
     uint32_t length;
-    uint32_t image;
+    // The claimed chunk: tiles [first, first + count) of the batch.
+    uint64_t chunk;
+    uint64_t first;
+    uint32_t count;
+    uint32_t image[kMaxChunk];  // image of each tile of the chunk
+    uint32_t length_of[kMaxChunk];
+    uint64_t offset[kMaxChunk]; // payload offset of each tile within its image's payload area
 };
 
+// Residual of a sample against its left neighbour: for uint16 the zigzag of the difference
+// taken as a signed 16-bit value, 2d for d >= 0 and -2d - 1 for d < 0 (encoder.cpp:32-37); for
+// FP32 words the XOR of the bit patterns.
 template <bool F32> __device__ __forceinline__ uint32_t residual(uint32_t cur, uint32_t prev) {
     if constexpr (F32) {
         return cur ^ prev;
     } else {
-        const uint32_t d = (cur - prev) & 0xffffu;
-        return d < 32768u ? d * 2u : (65536u - d) * 2u - 1u;
+        const int32_t d = static_cast<int16_t>(static_cast<uint16_t>(cur - prev));
+        return static_cast<uint32_t>((d * 2) ^ (d >> 31));
     }
 }
 
@@ -69,96 +83,128 @@ __device__ __forceinline__ void put_word(uint8_t *file, uint64_t byte, uint32_t 
     *reinterpret_cast<uint32_t *>(file + byte) = v;
 }
 
-// Word k of a PREDICT row of width w and residual width b: the bits [32 k, 32 k + 32) of the
-// packed residuals 1..w-1 (docs/format.md:77).
-__device__ __forceinline__ uint32_t packed_word(const uint32_t *res, uint32_t w, uint32_t b,
-                                                uint32_t k) {
-    if (b == 32) {
-        return res[1 + k];
-    }
-    const uint32_t first_bit = 32 * k;
-    const uint32_t count = w - 1;
-    const uint32_t j_end = (first_bit + 31) / b;
-    const uint32_t last = j_end < count - 1 ? j_end : count - 1;
-    uint32_t value = 0;
-    for (uint32_t j = first_bit / b; j <= last; ++j) {
-        const uint32_t pos = j * b;
-        const uint32_t r = res[1 + j];
-        value |= pos >= first_bit ? r << (pos - first_bit) : r >> (first_bit - pos);
-    }
-    return value;
+// Geometry of tile `index` of an image.
+struct TileGeom {
+    uint64_t x, y;
+    uint32_t w, h;
+};
+
+__device__ __forceinline__ TileGeom tile_geom(const tsk_encode_image &im, uint64_t index) {
+    TileGeom g;
+    g.x = (index % im.columns) * im.tile_width;
+    g.y = (index / im.columns) * im.tile_height;
+    g.w = static_cast<uint32_t>(im.width - g.x < im.tile_width ? im.width - g.x : im.tile_width);
+    g.h = static_cast<uint32_t>(im.height - g.y < im.tile_height ? im.height - g.y
+                                                                 : im.tile_height);
+    return g;
 }
 
-template <bool F32>
-__device__ void encode_tile(EncodeShared &sh, const tsk_encode_image &im, uint64_t index,
-                            uint64_t *flags, uint64_t global_tile, tsk_result *results,
-                            uint32_t image) {
-    const uint32_t warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-    const uint64_t x = (index % im.columns) * im.tile_width;
-    const uint64_t y = (index / im.columns) * im.tile_height;
-    const uint32_t w = static_cast<uint32_t>(im.width - x < im.tile_width ? im.width - x
-                                                                          : im.tile_width);
-    const uint32_t h = static_cast<uint32_t>(im.height - y < im.tile_height ? im.height - y
-                                                                            : im.tile_height);
-    constexpr uint32_t s = F32 ? 4 : 2;
-    const uint8_t *origin = reinterpret_cast<const uint8_t *>(im.input) + y * im.pitch + x * s;
+// Sample i of the tile in buffer `buf` (rows packed, w samples each).
+template <bool F32> __device__ __forceinline__ uint32_t px(const EncodeShared &sh, uint32_t buf,
+                                                            uint32_t i) {
+    if constexpr (F32) {
+        return sh.raw[buf][i];
+    } else {
+        return reinterpret_cast<const uint16_t *>(sh.raw[buf])[i];
+    }
+}
 
-    // 1. Pixels into shared memory, one warp per row; 16-byte loads when the row allows.
-    const bool vec = ((reinterpret_cast<uintptr_t>(origin) | im.pitch | (w * s)) & 15u) == 0;
-    for (uint32_t r = warp; r < h; r += kWarps) {
-        const uint8_t *line = origin + r * im.pitch;
-        uint32_t *dst = sh.px + r * w;
-        if (vec) {
-            constexpr uint32_t per = 16 / s;
-            for (uint32_t c = lane * per; c < w; c += 32 * per) {
-                const uint4 v = ld_nc_v4(line + c * s);
-                if constexpr (F32) {
-                    dst[c] = v.x;
-                    dst[c + 1] = v.y;
-                    dst[c + 2] = v.z;
-                    dst[c + 3] = v.w;
-                } else {
-                    const uint32_t q[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-                    for (uint32_t e = 0; e < 4; ++e) {
-                        dst[c + 2 * e] = q[e] & 0xffffu;
-                        dst[c + 2 * e + 1] = q[e] >> 16;
-                    }
-                }
-            }
-        } else {
-            for (uint32_t c = lane; c < w; c += 32) {
-                if constexpr (F32) {
-                    dst[c] = reinterpret_cast<const uint32_t *>(line)[c];
-                } else {
-                    dst[c] = reinterpret_cast<const uint16_t *>(line)[c];
-                }
+// Starts copying the tile's pixels into buffer `buf` and closes this thread's cp.async group.
+// Rows whose bytes are a multiple of 16 at 16-byte-aligned addresses go as 16-byte cp.async
+// copies issued by the whole CTA at once; other tiles are copied synchronously.
+template <bool F32>
+__device__ void issue_tile(EncodeShared &sh, uint32_t buf, const tsk_encode_image &im,
+                           const TileGeom &g) {
+    constexpr uint32_t s = F32 ? 4 : 2;
+    const uint32_t w = g.w, h = g.h;
+    const uint32_t row_bytes = w * s;
+    const uint8_t *origin = reinterpret_cast<const uint8_t *>(im.input) + g.y * im.pitch + g.x * s;
+    uint8_t *dst = reinterpret_cast<uint8_t *>(sh.raw[buf]);
+    if (((reinterpret_cast<uintptr_t>(origin) | im.pitch | row_bytes) & 15u) == 0) {
+        const uint32_t per_row = row_bytes / 16;
+        for (uint32_t c = threadIdx.x; c < h * per_row; c += kThreads) {
+            const uint32_t r = c / per_row, k = c - r * per_row;
+            cp_async16(dst + r * row_bytes + 16 * k, origin + r * im.pitch + 16 * k);
+        }
+    } else {
+        for (uint32_t i = threadIdx.x; i < w * h; i += kThreads) {
+            const uint32_t r = i / w, c = i - r * w;
+            const uint8_t *line = origin + r * im.pitch;
+            if constexpr (F32) {
+                sh.raw[buf][i] = reinterpret_cast<const uint32_t *>(line)[c];
+            } else {
+                reinterpret_cast<uint16_t *>(sh.raw[buf])[i] =
+                    reinterpret_cast<const uint16_t *>(line)[c];
             }
         }
     }
-    __syncthreads();
+    cp_async_commit();
+}
 
-    // 2. Residuals, row widths and the constant test.
-    const uint32_t first = sh.px[0];
-    bool constant = true;
-    for (uint32_t r = warp; r < h; r += kWarps) {
-        const uint32_t *line = sh.px + r * w;
-        uint32_t combined = 0;
-        for (uint32_t c = lane; c < w; c += 32) {
-            const uint32_t cur = line[c];
-            constant = constant && cur == first;
-            if (c != 0) {
-                const uint32_t z = residual<F32>(cur, line[c - 1]);
-                sh.res[r * w + c] = z;
-                combined |= z;
-            }
-        }
+__device__ __forceinline__ void issue_tile_any(EncodeShared &sh, uint32_t buf,
+                                               const tsk_encode_image &im, const TileGeom &g) {
+    if (im.type == 2) {
+        issue_tile<true>(sh, buf, im, g);
+    } else {
+        issue_tile<false>(sh, buf, im, g);
+    }
+}
+
+// This thread's part of a tile: kSeg consecutive samples of one row.
+constexpr uint32_t kSeg = 16;
+
+struct Segment {
+    uint32_t r, c0, n; // row, first column, samples (n = 0: no part)
+};
+
+__device__ __forceinline__ Segment segment_of(const TileGeom &g) {
+    const uint32_t per_row = (g.w + kSeg - 1) / kSeg;
+    Segment seg{0, 0, 0};
+    if (threadIdx.x < per_row * g.h) {
+        seg.r = threadIdx.x / per_row;
+        seg.c0 = (threadIdx.x - seg.r * per_row) * kSeg;
+        seg.n = g.w - seg.c0 < kSeg ? g.w - seg.c0 : kSeg;
+    }
+    return seg;
+}
+
+// The segment's residuals z[k] (column c0 + k; zero for column 0 and past the segment), their
+// OR, and whether every sample equals the tile's first sample.
+template <bool F32>
+__device__ __forceinline__ void segment_residuals(const EncodeShared &sh, uint32_t buf,
+                                                  const TileGeom &g, const Segment &seg,
+                                                  uint32_t (&z)[kSeg], uint32_t &orv,
+                                                  bool &constant) {
+    const uint32_t base = seg.r * g.w + seg.c0;
+    const uint32_t first = px<F32>(sh, buf, 0);
+    uint32_t prev = seg.c0 > 0 ? px<F32>(sh, buf, base - 1) : px<F32>(sh, buf, base);
+    orv = 0;
+    constant = true;
 #pragma unroll
-        for (uint32_t d = 16; d > 0; d >>= 1) {
-            combined |= __shfl_xor_sync(0xffffffffu, combined, d);
-        }
-        if (lane == 0) {
-            sh.bits[r] = 32u - __clz(combined);
+    for (uint32_t k = 0; k < kSeg; ++k) {
+        // Past the segment the previous sample repeats, so the residual is zero.
+        const uint32_t cur = k < seg.n ? px<F32>(sh, buf, base + k) : prev;
+        constant = constant && cur == first;
+        z[k] = residual<F32>(cur, prev); // column 0 compares the sample with itself: zero
+        orv |= z[k];
+        prev = cur;
+    }
+}
+
+// Row widths, the constant test, the row-cost scan and the canonical mode; sets sh.bits,
+// sh.row_word, sh.mode and sh.length. z keeps the segment's residuals for write_tile.
+template <bool F32>
+__device__ void analyze_tile(EncodeShared &sh, uint32_t buf, const TileGeom &g,
+                             const Segment &seg, uint32_t (&z)[kSeg]) {
+    const uint32_t warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    constexpr uint32_t s = F32 ? 4 : 2;
+    const uint32_t w = g.w, h = g.h;
+    uint32_t orv = 0;
+    bool constant = true;
+    if (seg.n != 0) {
+        segment_residuals<F32>(sh, buf, g, seg, z, orv, constant);
+        if (orv != 0) {
+            atomicOr(&sh.row_or[seg.r], orv);
         }
     }
     const bool uniform = __syncthreads_and(constant) != 0;
@@ -168,7 +214,12 @@ __device__ void encode_tile(EncodeShared &sh, const tsk_encode_image &im, uint64
         uint32_t carry = 0;
         for (uint32_t base = 0; base < h; base += 32) {
             const uint32_t r = base + lane;
-            const uint32_t cost = r < h ? 2u + ((w - 1) * sh.bits[r] + 31u) / 32u : 0u;
+            uint32_t cost = 0;
+            if (r < h) {
+                const uint32_t b = 32u - __clz(sh.row_or[r]);
+                sh.bits[r] = b;
+                cost = 2u + ((w - 1) * b + 31u) / 32u;
+            }
             uint32_t incl = cost;
 #pragma unroll
             for (uint32_t d = 1; d < 32; d <<= 1) {
@@ -195,50 +246,23 @@ __device__ void encode_tile(EncodeShared &sh, const tsk_encode_image &im, uint64
             }
             sh.mode = mode;
             sh.length = length;
-
-            // 3. Decoupled look-back over the earlier tiles of this image.
-            uint64_t *flag = flags + global_tile;
-            uint64_t prefix = 0;
-            if (index == 0) {
-                st_release(flag, kPrefix | length);
-            } else {
-                st_release(flag, kAggregate | length);
-                uint64_t j = global_tile - 1;
-                bool timed_out = false;
-                for (;;) {
-                    uint64_t v = ld_acquire(flags + j);
-                    uint32_t spins = 0;
-                    while ((v >> 62) == 0 && spins < (1u << 22)) {
-                        __nanosleep(64);
-                        v = ld_acquire(flags + j);
-                        ++spins;
-                    }
-                    if ((v >> 62) == 0) {
-                        timed_out = true;
-                        break;
-                    }
-                    prefix += v & kValue;
-                    if ((v >> 62) == 2) {
-                        break;
-                    }
-                    --j;
-                }
-                if (timed_out) {
-                    atomicCAS(&results[image].status, 0u, 9u);
-                }
-                st_release(flag, kPrefix | (prefix + length));
-            }
-            const uint64_t base = 64 + 32 * im.tile_count;
-            sh.offset = base + prefix;
-            sh.inclusive = prefix + length;
         }
     }
     __syncthreads();
+}
 
-    // 4. Index entry and payload, one writer per word.
+// Index entry and payload of an analysed tile, one writer per word; `offset` is the payload's
+// absolute position in the file. PREDICT rows are packed in shared memory first: each thread
+// appends its segment's residuals to the row's bit stream (docs/format.md:77) through a 64-bit
+// accumulator, OR-ing the words it touches, and the CTA then copies the payload out.
+template <bool F32>
+__device__ void write_tile(EncodeShared &sh, uint32_t buf, const tsk_encode_image &im,
+                           uint64_t index, const TileGeom &g, const Segment &seg,
+                           const uint32_t (&z)[kSeg], uint64_t offset) {
+    const uint32_t w = g.w, h = g.h;
     uint8_t *file = reinterpret_cast<uint8_t *>(im.output);
     const uint32_t mode = sh.mode, length = sh.length;
-    const uint64_t offset = sh.offset;
+    const uint32_t words = length / 4;
     if (threadIdx.x < 8) {
         uint32_t v = 0;
         switch (threadIdx.x) {
@@ -251,123 +275,350 @@ __device__ void encode_tile(EncodeShared &sh, const tsk_encode_image &im, uint64
         }
         put_word(file, 64 + 32 * index + 4 * threadIdx.x, v);
     }
-    const uint32_t words = length / 4;
     if (mode == TSK_RAW) {
-        const uint32_t count = w * h;
+        // The tile buffer holds the rows packed: it is the payload, zero-padded to a word.
+        const uint32_t bytes = w * h * (F32 ? 4 : 2);
         for (uint32_t k = threadIdx.x; k < words; k += kThreads) {
-            uint32_t v;
-            if constexpr (F32) {
-                v = sh.px[k];
-            } else {
-                const uint32_t i0 = 2 * k, i1 = 2 * k + 1;
-                v = sh.px[i0] | (i1 < count ? sh.px[i1] << 16 : 0u);
+            uint32_t v = sh.raw[buf][k];
+            if (4 * k + 4 > bytes) {
+                v &= 0xffffu; // an odd number of uint16 samples
             }
             put_word(file, offset + 4ull * k, v);
         }
-    } else if (mode == TSK_CONSTANT) {
+        return;
+    }
+    if (mode == TSK_CONSTANT) {
         if (threadIdx.x == 0) {
-            put_word(file, offset, first);
+            put_word(file, offset, px<F32>(sh, buf, 0));
         }
-    } else {
-        for (uint32_t k = threadIdx.x; k < words; k += kThreads) {
-            // Row of word k: the last row starting at or before it.
-            uint32_t lo = 0, hi = h;
-            while (hi - lo > 1) {
-                const uint32_t mid = (lo + hi) / 2;
-                if (sh.row_word[mid] <= k) {
-                    lo = mid;
-                } else {
-                    hi = mid;
+        return;
+    }
+    for (uint32_t k = threadIdx.x; k < words; k += kThreads) {
+        sh.stage[k] = 0;
+    }
+    __syncthreads();
+    if (seg.n != 0) {
+        const uint32_t r = seg.r, b = sh.bits[r], row = sh.row_word[r];
+        if (seg.c0 == 0) {
+            sh.stage[row] = px<F32>(sh, buf, r * w); // seed
+            sh.stage[row + 1] = b;                   // width word; reserved bytes zero
+        }
+        if (b != 0) {
+            // Residual j (column j + 1) starts at bit j * b of the row's packed words.
+            const uint32_t k0 = seg.c0 == 0 ? 1u : 0u;
+            const uint32_t start = (seg.c0 + k0 - 1) * b;
+            uint32_t bit = start & 31u;
+            uint32_t at = row + 2 + (start >> 5);
+            uint64_t acc = 0;
+#pragma unroll
+            for (uint32_t k = 0; k < kSeg; ++k) {
+                if (k >= k0 && k < seg.n) {
+                    acc |= static_cast<uint64_t>(z[k]) << bit;
+                    bit += b;
+                    if (bit >= 32) {
+                        atomicOr(&sh.stage[at], static_cast<uint32_t>(acc));
+                        acc >>= 32;
+                        bit -= 32;
+                        ++at;
+                    }
                 }
             }
-            const uint32_t local = k - sh.row_word[lo];
-            uint32_t v;
-            if (local == 0) {
-                v = sh.px[lo * w];
-            } else if (local == 1) {
-                v = sh.bits[lo];
-            } else {
-                v = packed_word(sh.res + lo * w, w, sh.bits[lo], local - 2);
+            if (bit != 0) {
+                atomicOr(&sh.stage[at], static_cast<uint32_t>(acc));
             }
-            put_word(file, offset + 4ull * k, v);
         }
     }
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < words; k += kThreads) {
+        put_word(file, offset + 4ull * k, sh.stage[k]);
+    }
+}
 
-    // 5. The last tile writes the header and the result.
-    if (index + 1 == im.tile_count && threadIdx.x < 16) {
-        const uint64_t size = 64 + 32 * im.tile_count + sh.inclusive;
-        uint32_t v = 0;
-        switch (threadIdx.x) {
-        case 0: v = 0x00435354u; break; // 'T' 'S' 'C' 0
-        case 1: v = 0x0a1a0a0du; break; // 13 10 26 10
-        case 2: v = 1u; break;          // version 1.0
-        case 3: v = 64u | (im.type << 16); break;
-        case 4: v = im.width; break;
-        case 5: v = im.height; break;
-        case 6: v = im.tile_width | (static_cast<uint32_t>(im.tile_height) << 16); break;
-        case 7: v = 32u; break;
-        case 8: v = static_cast<uint32_t>(im.tile_count); break;
-        case 9: v = static_cast<uint32_t>(im.tile_count >> 32); break;
-        case 10: v = 64u; break;
-        case 11: v = 0u; break;
-        case 12: v = static_cast<uint32_t>(64 + 32 * im.tile_count); break;
-        case 13: v = static_cast<uint32_t>((64 + 32 * im.tile_count) >> 32); break;
-        case 14: v = static_cast<uint32_t>(size); break;
-        default: v = static_cast<uint32_t>(size >> 32); break;
+// The 64-byte header of a finished image (threads 0-15) and its result record.
+__device__ void write_header(const tsk_encode_image &im, uint64_t payload_bytes,
+                             tsk_result *result) {
+    if (threadIdx.x >= 16) {
+        return;
+    }
+    uint8_t *file = reinterpret_cast<uint8_t *>(im.output);
+    const uint64_t size = 64 + 32 * im.tile_count + payload_bytes;
+    uint32_t v = 0;
+    switch (threadIdx.x) {
+    case 0: v = 0x00435354u; break; // 'T' 'S' 'C' 0
+    case 1: v = 0x0a1a0a0du; break; // 13 10 26 10
+    case 2: v = 1u; break;          // version 1.0
+    case 3: v = 64u | (im.type << 16); break;
+    case 4: v = im.width; break;
+    case 5: v = im.height; break;
+    case 6: v = im.tile_width | (static_cast<uint32_t>(im.tile_height) << 16); break;
+    case 7: v = 32u; break;
+    case 8: v = static_cast<uint32_t>(im.tile_count); break;
+    case 9: v = static_cast<uint32_t>(im.tile_count >> 32); break;
+    case 10: v = 64u; break;
+    case 11: v = 0u; break;
+    case 12: v = static_cast<uint32_t>(64 + 32 * im.tile_count); break;
+    case 13: v = static_cast<uint32_t>((64 + 32 * im.tile_count) >> 32); break;
+    case 14: v = static_cast<uint32_t>(size); break;
+    default: v = static_cast<uint32_t>(size >> 32); break;
+    }
+    put_word(file, 4 * threadIdx.x, v);
+    if (threadIdx.x == 0) {
+        // The launcher cleared the record; a look-back timeout may have set cuda_error.
+        result->bytes_written = size;
+    }
+}
+
+// Sum over the warp of a 64-bit value (every lane gets it).
+__device__ __forceinline__ uint64_t warp_sum64(uint64_t v) {
+#pragma unroll
+    for (uint32_t d = 16; d > 0; d >>= 1) {
+        v += __shfl_xor_sync(0xffffffffu, v, d);
+    }
+    return v;
+}
+
+// Images of a batch: a table (plans) or one image passed by value (allocation-free path).
+struct ImageTable {
+    const tsk_encode_image *images;
+    uint32_t count;
+    __device__ const tsk_encode_image &operator[](uint32_t i) const {
+        return images[i];
+    }
+    // The image owning batch tile `id`: the last image whose first tile is at or before it.
+    __device__ uint32_t owner(uint64_t id) const {
+        uint32_t lo = 0, hi = count;
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) / 2;
+            if (images[mid].first_tile <= id) {
+                lo = mid;
+            } else {
+                hi = mid;
+            }
         }
-        put_word(file, 4 * threadIdx.x, v);
+        return lo;
+    }
+};
+
+struct SingleImage {
+    const tsk_encode_image *image;
+    __device__ const tsk_encode_image &operator[](uint32_t) const {
+        return *image;
+    }
+    __device__ uint32_t owner(uint64_t) const {
+        return 0;
+    }
+};
+
+// Looks back over chunks [stop, g) (all of them inside one image) from chunk g - 1 downwards,
+// 32 per step, and returns the summed lengths up to the nearest inclusive prefix. Warp 0 only.
+__device__ uint64_t look_back(const uint64_t *flags, uint64_t g, uint64_t stop, bool &timed_out) {
+    const uint32_t lane = threadIdx.x % 32;
+    uint64_t carry = 0;
+    int64_t j = static_cast<int64_t>(g) - 1;
+    for (;;) {
+        const int64_t idx = j - lane;
+        uint64_t v = kPrefix; // chunks before the image's first one end the walk with nothing
+        if (idx >= static_cast<int64_t>(stop)) {
+            v = ld_acquire(flags + idx);
+            uint32_t spins = 0;
+            while ((v >> 62) == 0 && spins < (1u << 22)) {
+                __nanosleep(64);
+                v = ld_acquire(flags + idx);
+                ++spins;
+            }
+            if ((v >> 62) == 0) {
+                timed_out = true;
+                v = kPrefix;
+            }
+        }
+        const uint32_t prefixes = __ballot_sync(0xffffffffu, (v >> 62) == 2);
+        const uint32_t upto = prefixes != 0 ? __ffs(prefixes) - 1 : 31u;
+        carry += warp_sum64(lane <= upto ? (v & kValue) : 0ull);
+        if (prefixes != 0) {
+            break;
+        }
+        j -= 32;
+    }
+    timed_out = __any_sync(0xffffffffu, timed_out);
+    return carry;
+}
+
+// The persistent loop: claim a chunk, analyse its tiles, publish, look back, write.
+template <typename Images>
+__device__ void encode_chunks(EncodeShared &sh, const Images &images, uint64_t total_tiles,
+                              uint32_t chunk_tiles, uint64_t *state, tsk_result *results) {
+    uint64_t *counter = state;
+    uint64_t *flags = state + 2;
+    const uint32_t warp = threadIdx.x / 32;
+    for (;;) {
         if (threadIdx.x == 0) {
-            // The launcher cleared the records; a look-back timeout may have set cuda_error.
-            results[image].bytes_written = size;
+            const uint64_t g = atomicAdd(reinterpret_cast<unsigned long long *>(counter), 1ull);
+            const uint64_t first = g * chunk_tiles;
+            sh.chunk = g;
+            sh.first = first;
+            sh.count = first < total_tiles
+                           ? static_cast<uint32_t>(total_tiles - first < chunk_tiles
+                                                       ? total_tiles - first
+                                                       : chunk_tiles)
+                           : 0u;
         }
+        __syncthreads();
+        const uint32_t count = sh.count;
+        if (count == 0) {
+            return;
+        }
+        const uint64_t g = sh.chunk, first = sh.first;
+        if (threadIdx.x < count) {
+            sh.image[threadIdx.x] = images.owner(first + threadIdx.x);
+        }
+        if (threadIdx.x < TSK_MAX_ROWS) {
+            sh.row_or[threadIdx.x] = 0;
+        }
+        __syncthreads();
+
+        // Tile i of the chunk: its image and its geometry.
+        auto tile = [&](uint32_t i, const tsk_encode_image *&im, uint64_t &index) {
+            im = &images[sh.image[i]];
+            index = first + i - im->first_tile;
+            return tile_geom(*im, index);
+        };
+        // Copies tile i into buffer i % 2 (a cp.async group is closed either way).
+        auto prefetch = [&](uint32_t i) {
+            if (i < count) {
+                const tsk_encode_image *im;
+                uint64_t index;
+                const TileGeom geom = tile(i, im, index);
+                issue_tile_any(sh, i % 2, *im, geom);
+            } else {
+                cp_async_commit();
+            }
+        };
+
+        // 1. Lengths of the chunk's tiles; tile i + 1 is copied while tile i is analysed.
+        prefetch(0);
+        for (uint32_t i = 0; i < count; ++i) {
+            prefetch(i + 1);
+            cp_async_wait<1>();
+            __syncthreads();
+            const tsk_encode_image *im;
+            uint64_t index;
+            const TileGeom geom = tile(i, im, index);
+            const Segment seg = segment_of(geom);
+            uint32_t z[kSeg];
+            if (im->type == 2) {
+                analyze_tile<true>(sh, i % 2, geom, seg, z);
+            } else {
+                analyze_tile<false>(sh, i % 2, geom, seg, z);
+            }
+            if (threadIdx.x == 0) {
+                sh.length_of[i] = sh.length;
+            }
+            if (threadIdx.x < TSK_MAX_ROWS) {
+                sh.row_or[threadIdx.x] = 0; // for the next tile (read before the last barrier)
+            }
+        }
+        // The first tile's copy for step 3 flies during the look-back.
+        prefetch(0);
+        __syncthreads();
+
+        // 2. Offsets: within the chunk, then the carry of the first image from earlier chunks.
+        if (warp == 0) {
+            const uint32_t lane = threadIdx.x % 32;
+            const uint32_t first_image = sh.image[0], last_image = sh.image[count - 1];
+            uint64_t tail = 0; // lengths of the last image's tiles in this chunk
+            if (lane == 0) {
+                uint64_t run = 0;
+                for (uint32_t i = 0; i < count; ++i) {
+                    if (i != 0 && sh.image[i] != sh.image[i - 1]) {
+                        run = 0;
+                    }
+                    sh.offset[i] = run;
+                    run += sh.length_of[i];
+                }
+                tail = run;
+            }
+            __syncwarp();
+            tail = __shfl_sync(0xffffffffu, tail, 0);
+            const uint64_t image_first = images[first_image].first_tile;
+            const bool carried = image_first < first; // the first image began in an earlier chunk
+            if (lane == 0) {
+                // The last image's inclusive prefix at the end of this chunk is already known
+                // unless it is the first image and that began earlier: then only its sum is.
+                const bool known = !carried || first_image != last_image;
+                st_release(flags + g, (known ? kPrefix : kAggregate) | tail);
+            }
+            uint64_t carry = 0;
+            if (carried) {
+                bool timed_out = false;
+                carry = look_back(flags, g, image_first / chunk_tiles, timed_out);
+                if (lane == 0) {
+                    if (first_image == last_image) {
+                        st_release(flags + g, kPrefix | (carry + tail));
+                    }
+                    if (timed_out) {
+                        atomicCAS(&results[first_image].status, 0u, 9u);
+                    }
+                }
+            }
+            __syncwarp();
+            if (lane < count && sh.image[lane] == first_image) {
+                sh.offset[lane] += carry;
+            }
+        }
+        __syncthreads();
+
+        // 3. Index entries and payloads; the last tile of an image writes its header.
+        for (uint32_t i = 0; i < count; ++i) {
+            prefetch(i + 1);
+            cp_async_wait<1>();
+            __syncthreads();
+            const uint32_t m = sh.image[i];
+            const tsk_encode_image *im;
+            uint64_t index;
+            const TileGeom geom = tile(i, im, index);
+            const uint64_t offset = 64 + 32 * im->tile_count + sh.offset[i];
+            const Segment seg = segment_of(geom);
+            uint32_t z[kSeg];
+            if (im->type == 2) {
+                analyze_tile<true>(sh, i % 2, geom, seg, z);
+                write_tile<true>(sh, i % 2, *im, index, geom, seg, z, offset);
+            } else {
+                analyze_tile<false>(sh, i % 2, geom, seg, z);
+                write_tile<false>(sh, i % 2, *im, index, geom, seg, z, offset);
+            }
+            if (threadIdx.x < TSK_MAX_ROWS) {
+                sh.row_or[threadIdx.x] = 0; // for the next tile (read before the last barrier)
+            }
+            if (index + 1 == im->tile_count) {
+                write_header(*im, sh.offset[i] + sh.length_of[i], results + m);
+            }
+            __syncthreads();
+        }
+        cp_async_wait<0>();
     }
 }
 
 __global__ void __launch_bounds__(kThreads)
     encode_kernel(const tsk_encode_image *__restrict__ images, uint32_t image_count,
-                  uint64_t total_tiles, uint64_t *state, tsk_result *results) {
+                  uint64_t total_tiles, uint32_t chunk_tiles, uint64_t *state,
+                  tsk_result *results) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
     EncodeShared &sh = *reinterpret_cast<EncodeShared *>(smem_raw);
-    uint64_t *counter = state;
-    uint64_t *flags = state + 2;
-    for (;;) {
-        if (threadIdx.x == 0) {
-            const uint64_t id = atomicAdd(reinterpret_cast<unsigned long long *>(counter), 1ull);
-            sh.tile_id = id < total_tiles ? id : total_tiles;
-            // Image owning tile id: the last image whose first tile is at or before it.
-            uint32_t lo = 0, hi = image_count;
-            while (hi - lo > 1) {
-                const uint32_t mid = (lo + hi) / 2;
-                if (images[mid].first_tile <= id) {
-                    lo = mid;
-                } else {
-                    hi = mid;
-                }
-            }
-            sh.image = lo;
-        }
-        __syncthreads();
-        const uint64_t id = sh.tile_id;
-        const uint32_t image = sh.image;
-        if (id >= total_tiles) {
-            return;
-        }
-        const tsk_encode_image &im = images[image];
-        const uint64_t index = id - im.first_tile;
-        if (im.type == 2) {
-            encode_tile<true>(sh, im, index, flags, id, results, image);
-        } else {
-            encode_tile<false>(sh, im, index, flags, id, results, image);
-        }
-        __syncthreads();
-    }
+    encode_chunks(sh, ImageTable{images, image_count}, total_tiles, chunk_tiles, state, results);
+}
+
+// Tiles per chunk for a launch of `grid` CTAs: as many as spread the tiles over the grid in one
+// round, at most kMaxChunk (larger batches take several rounds).
+uint32_t chunk_tiles_for(uint64_t total_tiles, uint64_t grid) {
+    const uint64_t k = (total_tiles + grid - 1) / grid;
+    return static_cast<uint32_t>(k < 1 ? 1 : (k > kMaxChunk ? kMaxChunk : k));
 }
 
 } // namespace
 } // namespace tsk
 
 extern "C" uint64_t tsk_encode_state_bytes(uint64_t total_tiles) {
-    return 8 * (total_tiles + 2);
+    return 8 * (total_tiles + 2); // the chunk counter, a spare word, one flag per chunk at most
 }
 
 extern "C" int tsk_encode_prepare(int device) {
@@ -399,9 +650,11 @@ extern "C" int tsk_encode_launch(const tsk_encode_image *images, uint32_t image_
                                                       smem);
     if (e != cudaSuccess) return e;
     uint64_t grid = static_cast<uint64_t>(sms) * (per_sm > 0 ? per_sm : 1);
-    if (grid > total_tiles) grid = total_tiles;
+    const uint32_t k = tsk::chunk_tiles_for(total_tiles, grid);
+    const uint64_t chunks = (total_tiles + k - 1) / k;
+    if (grid > chunks) grid = chunks;
     tsk::encode_kernel<<<static_cast<uint32_t>(grid), tsk::kThreads, smem, stream>>>(
-        images, image_count, total_tiles, static_cast<uint64_t *>(state), results);
+        images, image_count, total_tiles, k, static_cast<uint64_t *>(state), results);
     return cudaGetLastError();
 }
 
@@ -429,30 +682,11 @@ constexpr uint64_t kStaticStateWords = 131072;
 __device__ __align__(256) uint64_t g_encode_scratch[kStaticStateWords];
 
 __global__ void __launch_bounds__(kThreads)
-    encode_kernel_static(tsk_encode_image image, uint64_t total_tiles, uint64_t *state,
-                         tsk_result *result) {
+    encode_kernel_static(const __grid_constant__ tsk_encode_image image, uint64_t total_tiles,
+                         uint32_t chunk_tiles, uint64_t *state, tsk_result *result) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
     EncodeShared &sh = *reinterpret_cast<EncodeShared *>(smem_raw);
-    uint64_t *counter = state;
-    uint64_t *flags = state + 2;
-    for (;;) {
-        if (threadIdx.x == 0) {
-            const uint64_t id = atomicAdd(reinterpret_cast<unsigned long long *>(counter), 1ull);
-            sh.tile_id = id < total_tiles ? id : total_tiles;
-            sh.image = 0;
-        }
-        __syncthreads();
-        const uint64_t id = sh.tile_id;
-        if (id >= total_tiles) {
-            return;
-        }
-        if (image.type == 2) {
-            encode_tile<true>(sh, image, id, flags, id, result, 0);
-        } else {
-            encode_tile<false>(sh, image, id, flags, id, result, 0);
-        }
-        __syncthreads();
-    }
+    encode_chunks(sh, SingleImage{&image}, total_tiles, chunk_tiles, state, result);
 }
 
 // Per-device set-up, done by the first call on each device with that device current.
@@ -516,9 +750,11 @@ extern "C" int tsk_encode_static_launch(const tsk_encode_image *image, tsk_resul
     if (e != cudaSuccess) return e;
     e = cudaMemsetAsync(result, 0, sizeof(tsk_result), stream);
     if (e != cudaSuccess) return e;
-    const uint64_t grid = setup.grid < total ? setup.grid : total;
+    const uint32_t k = tsk::chunk_tiles_for(total, setup.grid);
+    const uint64_t chunks = (total + k - 1) / k;
+    const uint64_t grid = setup.grid < chunks ? setup.grid : chunks;
     tsk::encode_kernel_static<<<static_cast<uint32_t>(grid), tsk::kThreads,
-                                sizeof(tsk::EncodeShared), stream>>>(*image, total, setup.scratch,
-                                                                     result);
+                                sizeof(tsk::EncodeShared), stream>>>(*image, total, k,
+                                                                     setup.scratch, result);
     return cudaGetLastError();
 }

@@ -77,6 +77,19 @@ __device__ __forceinline__ void cp_async4(void *dst, const void *src) {
                  : "memory");
 }
 
+// 16-byte asynchronous copy global -> shared (both 16-byte aligned), in this thread's current
+// cp.async group; commit closes the group, wait<N> waits until at most N groups are pending.
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N> __device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 // The barrier receives one more arrival once all of this thread's earlier cp.async copies have
 // landed (the pending count is raised first, so the phase cannot complete before them).
 __device__ __forceinline__ void cp_async_arrive(uint64_t *bar) {
