@@ -922,7 +922,8 @@ Status compress_async(const BatchPlan &plan, MutableBytes workspace, ResultBuffe
     }
     void *state = static_cast<std::uint8_t *>(workspace.data) + p->layout.temp;
     return detail::cuda_status(tsk_encode_launch(
-        p->encode_images, static_cast<std::uint32_t>(p->count), p->total_tiles, 0, state,
+        p->encode_images, static_cast<std::uint32_t>(p->count), p->total_tiles,
+        p->type == PixelType::float32 ? 1u : 0u, state,
         reinterpret_cast<tsk_result *>(results.data), stream), "encode launch");
 }
 

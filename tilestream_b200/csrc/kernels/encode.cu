@@ -38,11 +38,35 @@ constexpr uint64_t kValue = (1ull << 62) - 1;
 
 constexpr uint32_t kMaxChunk = 8;
 
-struct EncodeShared {
+// Divides small numerators (n * d < 2^32) by d with a multiply: floor(n / d) equals the high
+// word of n * ceil(2^32 / d).
+struct Divider {
+    uint32_t d, magic;
+    __device__ static Divider of(uint32_t d) {
+        return {d, d > 1 ? 0xffffffffu / d + 1u : 0u};
+    }
+    __device__ __forceinline__ uint32_t div(uint32_t n) const {
+        return d > 1 ? __umulhi(n, magic) : n;
+    }
+};
+
+// One tile of a chunk, computed once when the chunk is claimed: its position in its image and
+// the divisors of its copy and segment layouts.
+struct TileGeom {
+    uint64_t x, y;
+    uint64_t index; // tile index within its image
+    uint32_t w, h;
+    Divider vec_per_row; // 16-byte pieces per row (when rows are 16-byte multiples)
+    Divider seg_per_row; // thread segments per row
+};
+
+// Words: the largest tile in 32-bit words, 2048 for uint16-only batches (4096 samples) and
+// 4096 when the batch has FP32 images; a PREDICT payload is always shorter than the RAW one.
+template <uint32_t Words> struct EncodeShared {
     // Two tile buffers: the tile being analysed and the next one in flight. Rows are packed
     // (w samples each), as uint16 or FP32 words.
-    alignas(16) uint32_t raw[2][TSK_TILE_PIXELS];
-    uint32_t stage[TSK_PAYLOAD_BYTES / 4]; // the tile payload being written (PREDICT)
+    alignas(16) uint32_t raw[2][Words];
+    uint32_t stage[Words]; // the tile payload being written (PREDICT)
     uint32_t row_or[TSK_MAX_ROWS];         // OR of each row's residuals
     uint32_t bits[TSK_MAX_ROWS];
     uint32_t row_word[TSK_MAX_ROWS + 1]; // first payload word of each row
@@ -53,6 +77,7 @@ struct EncodeShared {
     uint64_t first;
     uint32_t count;
     uint32_t image[kMaxChunk];  // image of each tile of the chunk
+    TileGeom geom[kMaxChunk];
     uint32_t length_of[kMaxChunk];
     uint64_t offset[kMaxChunk]; // payload offset of each tile within its image's payload area
 };
@@ -83,25 +108,23 @@ __device__ __forceinline__ void put_word(uint8_t *file, uint64_t byte, uint32_t 
     *reinterpret_cast<uint32_t *>(file + byte) = v;
 }
 
-// Geometry of tile `index` of an image.
-struct TileGeom {
-    uint64_t x, y;
-    uint32_t w, h;
-};
-
-__device__ __forceinline__ TileGeom tile_geom(const tsk_encode_image &im, uint64_t index) {
+__device__ TileGeom tile_geom(const tsk_encode_image &im, uint64_t index) {
     TileGeom g;
+    g.index = index;
     g.x = (index % im.columns) * im.tile_width;
     g.y = (index / im.columns) * im.tile_height;
     g.w = static_cast<uint32_t>(im.width - g.x < im.tile_width ? im.width - g.x : im.tile_width);
     g.h = static_cast<uint32_t>(im.height - g.y < im.tile_height ? im.height - g.y
                                                                  : im.tile_height);
+    const uint32_t s = im.type == 2 ? 4 : 2;
+    g.vec_per_row = Divider::of((g.w * s) / 16 != 0 ? (g.w * s) / 16 : 1);
+    g.seg_per_row = Divider::of((g.w + 15) / 16);
     return g;
 }
 
 // Sample i of the tile in buffer `buf` (rows packed, w samples each).
-template <bool F32> __device__ __forceinline__ uint32_t px(const EncodeShared &sh, uint32_t buf,
-                                                            uint32_t i) {
+template <bool F32, typename Sh>
+__device__ __forceinline__ uint32_t px(const Sh &sh, uint32_t buf, uint32_t i) {
     if constexpr (F32) {
         return sh.raw[buf][i];
     } else {
@@ -112,9 +135,8 @@ template <bool F32> __device__ __forceinline__ uint32_t px(const EncodeShared &s
 // Starts copying the tile's pixels into buffer `buf` and closes this thread's cp.async group.
 // Rows whose bytes are a multiple of 16 at 16-byte-aligned addresses go as 16-byte cp.async
 // copies issued by the whole CTA at once; other tiles are copied synchronously.
-template <bool F32>
-__device__ void issue_tile(EncodeShared &sh, uint32_t buf, const tsk_encode_image &im,
-                           const TileGeom &g) {
+template <bool F32, typename Sh>
+__device__ void issue_tile(Sh &sh, uint32_t buf, const tsk_encode_image &im, const TileGeom &g) {
     constexpr uint32_t s = F32 ? 4 : 2;
     const uint32_t w = g.w, h = g.h;
     const uint32_t row_bytes = w * s;
@@ -123,7 +145,7 @@ __device__ void issue_tile(EncodeShared &sh, uint32_t buf, const tsk_encode_imag
     if (((reinterpret_cast<uintptr_t>(origin) | im.pitch | row_bytes) & 15u) == 0) {
         const uint32_t per_row = row_bytes / 16;
         for (uint32_t c = threadIdx.x; c < h * per_row; c += kThreads) {
-            const uint32_t r = c / per_row, k = c - r * per_row;
+            const uint32_t r = g.vec_per_row.div(c), k = c - r * per_row;
             cp_async16(dst + r * row_bytes + 16 * k, origin + r * im.pitch + 16 * k);
         }
     } else {
@@ -141,9 +163,10 @@ __device__ void issue_tile(EncodeShared &sh, uint32_t buf, const tsk_encode_imag
     cp_async_commit();
 }
 
-__device__ __forceinline__ void issue_tile_any(EncodeShared &sh, uint32_t buf,
-                                               const tsk_encode_image &im, const TileGeom &g) {
-    if (im.type == 2) {
+template <bool AnyF32, typename Sh>
+__device__ __forceinline__ void issue_tile_any(Sh &sh, uint32_t buf, const tsk_encode_image &im,
+                                               const TileGeom &g) {
+    if (AnyF32 && im.type == 2) {
         issue_tile<true>(sh, buf, im, g);
     } else {
         issue_tile<false>(sh, buf, im, g);
@@ -158,10 +181,10 @@ struct Segment {
 };
 
 __device__ __forceinline__ Segment segment_of(const TileGeom &g) {
-    const uint32_t per_row = (g.w + kSeg - 1) / kSeg;
+    const uint32_t per_row = g.seg_per_row.d;
     Segment seg{0, 0, 0};
     if (threadIdx.x < per_row * g.h) {
-        seg.r = threadIdx.x / per_row;
+        seg.r = g.seg_per_row.div(threadIdx.x);
         seg.c0 = (threadIdx.x - seg.r * per_row) * kSeg;
         seg.n = g.w - seg.c0 < kSeg ? g.w - seg.c0 : kSeg;
     }
@@ -169,45 +192,74 @@ __device__ __forceinline__ Segment segment_of(const TileGeom &g) {
 }
 
 // The segment's residuals z[k] (column c0 + k; zero for column 0 and past the segment), their
-// OR, and whether every sample equals the tile's first sample.
-template <bool F32>
-__device__ __forceinline__ void segment_residuals(const EncodeShared &sh, uint32_t buf,
+// OR, and its first sample.
+template <bool F32, typename Sh>
+__device__ __forceinline__ void segment_residuals(const Sh &sh, uint32_t buf,
                                                   const TileGeom &g, const Segment &seg,
                                                   uint32_t (&z)[kSeg], uint32_t &orv,
-                                                  bool &constant) {
+                                                  uint32_t &head) {
     const uint32_t base = seg.r * g.w + seg.c0;
-    const uint32_t first = px<F32>(sh, buf, 0);
-    uint32_t prev = seg.c0 > 0 ? px<F32>(sh, buf, base - 1) : px<F32>(sh, buf, base);
+    uint32_t x[kSeg];
+    // A whole segment of a row that starts on 16 bytes is read with 16-byte loads (neighbouring
+    // threads' segments are 32 or 64 bytes apart, so sample-by-sample reads conflict on banks).
+    constexpr uint32_t kPerVec = F32 ? 4 : 8;
+    if (seg.n == kSeg && g.w % kPerVec == 0) {
+        const uint4 *v = reinterpret_cast<const uint4 *>(sh.raw[buf]) + base / kPerVec;
+#pragma unroll
+        for (uint32_t q = 0; q < kSeg / kPerVec; ++q) {
+            const uint4 u = v[q];
+            if constexpr (F32) {
+                x[4 * q] = u.x;
+                x[4 * q + 1] = u.y;
+                x[4 * q + 2] = u.z;
+                x[4 * q + 3] = u.w;
+            } else {
+                const uint32_t wd[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+                for (uint32_t e = 0; e < 4; ++e) {
+                    x[8 * q + 2 * e] = wd[e] & 0xffffu;
+                    x[8 * q + 2 * e + 1] = wd[e] >> 16;
+                }
+            }
+        }
+    } else {
+#pragma unroll
+        for (uint32_t k = 0; k < kSeg; ++k) {
+            // Past the segment the last sample repeats, so the residual is zero.
+            x[k] = px<F32>(sh, buf, base + (k < seg.n ? k : seg.n - 1));
+        }
+    }
+    uint32_t prev = seg.c0 > 0 ? px<F32>(sh, buf, base - 1) : x[0];
+    head = x[0];
     orv = 0;
-    constant = true;
 #pragma unroll
     for (uint32_t k = 0; k < kSeg; ++k) {
-        // Past the segment the previous sample repeats, so the residual is zero.
-        const uint32_t cur = k < seg.n ? px<F32>(sh, buf, base + k) : prev;
-        constant = constant && cur == first;
-        z[k] = residual<F32>(cur, prev); // column 0 compares the sample with itself: zero
+        z[k] = residual<F32>(x[k], prev); // column 0 compares the sample with itself: zero
         orv |= z[k];
-        prev = cur;
+        prev = x[k];
     }
 }
 
 // Row widths, the constant test, the row-cost scan and the canonical mode; sets sh.bits,
 // sh.row_word, sh.mode and sh.length. z keeps the segment's residuals for write_tile.
-template <bool F32>
-__device__ void analyze_tile(EncodeShared &sh, uint32_t buf, const TileGeom &g,
+template <bool F32, typename Sh>
+__device__ void analyze_tile(Sh &sh, uint32_t buf, const TileGeom &g,
                              const Segment &seg, uint32_t (&z)[kSeg]) {
     const uint32_t warp = threadIdx.x / 32, lane = threadIdx.x % 32;
     constexpr uint32_t s = F32 ? 4 : 2;
     const uint32_t w = g.w, h = g.h;
-    uint32_t orv = 0;
-    bool constant = true;
+    // The tile is constant when every row starts with the tile's first sample and no row has a
+    // nonzero residual.
+    uint32_t orv = 0, head = 0;
+    bool seed_ok = true;
     if (seg.n != 0) {
-        segment_residuals<F32>(sh, buf, g, seg, z, orv, constant);
+        segment_residuals<F32>(sh, buf, g, seg, z, orv, head);
         if (orv != 0) {
             atomicOr(&sh.row_or[seg.r], orv);
         }
+        seed_ok = seg.c0 != 0 || head == px<F32>(sh, buf, 0);
     }
-    const bool uniform = __syncthreads_and(constant) != 0;
+    bool uniform = __syncthreads_and(seed_ok) != 0;
 
     // Row costs in words (descriptor + packed residuals), scanned by warp 0.
     if (warp == 0) {
@@ -220,6 +272,7 @@ __device__ void analyze_tile(EncodeShared &sh, uint32_t buf, const TileGeom &g,
                 sh.bits[r] = b;
                 cost = 2u + ((w - 1) * b + 31u) / 32u;
             }
+            uniform = __all_sync(0xffffffffu, uniform && (r >= h || sh.row_or[r] == 0));
             uint32_t incl = cost;
 #pragma unroll
             for (uint32_t d = 1; d < 32; d <<= 1) {
@@ -255,8 +308,8 @@ __device__ void analyze_tile(EncodeShared &sh, uint32_t buf, const TileGeom &g,
 // absolute position in the file. PREDICT rows are packed in shared memory first: each thread
 // appends its segment's residuals to the row's bit stream (docs/format.md:77) through a 64-bit
 // accumulator, OR-ing the words it touches, and the CTA then copies the payload out.
-template <bool F32>
-__device__ void write_tile(EncodeShared &sh, uint32_t buf, const tsk_encode_image &im,
+template <bool F32, typename Sh>
+__device__ void write_tile(Sh &sh, uint32_t buf, const tsk_encode_image &im,
                            uint64_t index, const TileGeom &g, const Segment &seg,
                            const uint32_t (&z)[kSeg], uint64_t offset) {
     const uint32_t w = g.w, h = g.h;
@@ -310,16 +363,37 @@ __device__ void write_tile(EncodeShared &sh, uint32_t buf, const tsk_encode_imag
             uint32_t bit = start & 31u;
             uint32_t at = row + 2 + (start >> 5);
             uint64_t acc = 0;
+            // Appends `bits` bits of v (bits <= 32) and flushes a full word.
+            auto append = [&](uint32_t v, uint32_t bits) {
+                acc |= static_cast<uint64_t>(v) << bit;
+                bit += bits;
+                if (bit >= 32) {
+                    atomicOr(&sh.stage[at], static_cast<uint32_t>(acc));
+                    acc >>= 32;
+                    bit -= 32;
+                    ++at;
+                }
+            };
+            if (!F32 && seg.n == kSeg) {
+                // uint16 (b <= 16): two residuals joined into one 2b-bit value per append.
+                const uint32_t scale = 1u << b;
+                if (k0 == 0) {
 #pragma unroll
-            for (uint32_t k = 0; k < kSeg; ++k) {
-                if (k >= k0 && k < seg.n) {
-                    acc |= static_cast<uint64_t>(z[k]) << bit;
-                    bit += b;
-                    if (bit >= 32) {
-                        atomicOr(&sh.stage[at], static_cast<uint32_t>(acc));
-                        acc >>= 32;
-                        bit -= 32;
-                        ++at;
+                    for (uint32_t k = 0; k < kSeg; k += 2) {
+                        append(z[k] + z[k + 1] * scale, 2 * b);
+                    }
+                } else {
+#pragma unroll
+                    for (uint32_t k = 1; k + 1 < kSeg; k += 2) {
+                        append(z[k] + z[k + 1] * scale, 2 * b);
+                    }
+                    append(z[kSeg - 1], b);
+                }
+            } else {
+#pragma unroll
+                for (uint32_t k = 0; k < kSeg; ++k) {
+                    if (k >= k0 && k < seg.n) {
+                        append(z[k], b);
                     }
                 }
             }
@@ -444,8 +518,8 @@ __device__ uint64_t look_back(const uint64_t *flags, uint64_t g, uint64_t stop, 
 }
 
 // The persistent loop: claim a chunk, analyse its tiles, publish, look back, write.
-template <typename Images>
-__device__ void encode_chunks(EncodeShared &sh, const Images &images, uint64_t total_tiles,
+template <bool AnyF32, typename Sh, typename Images>
+__device__ void encode_chunks(Sh &sh, const Images &images, uint64_t total_tiles,
                               uint32_t chunk_tiles, uint64_t *state, tsk_result *results) {
     uint64_t *counter = state;
     uint64_t *flags = state + 2;
@@ -469,7 +543,9 @@ __device__ void encode_chunks(EncodeShared &sh, const Images &images, uint64_t t
         }
         const uint64_t g = sh.chunk, first = sh.first;
         if (threadIdx.x < count) {
-            sh.image[threadIdx.x] = images.owner(first + threadIdx.x);
+            const uint32_t m = images.owner(first + threadIdx.x);
+            sh.image[threadIdx.x] = m;
+            sh.geom[threadIdx.x] = tile_geom(images[m], first + threadIdx.x - images[m].first_tile);
         }
         if (threadIdx.x < TSK_MAX_ROWS) {
             sh.row_or[threadIdx.x] = 0;
@@ -477,18 +553,19 @@ __device__ void encode_chunks(EncodeShared &sh, const Images &images, uint64_t t
         __syncthreads();
 
         // Tile i of the chunk: its image and its geometry.
-        auto tile = [&](uint32_t i, const tsk_encode_image *&im, uint64_t &index) {
+        auto tile = [&](uint32_t i, const tsk_encode_image *&im,
+                        uint64_t &index) -> const TileGeom & {
             im = &images[sh.image[i]];
-            index = first + i - im->first_tile;
-            return tile_geom(*im, index);
+            index = sh.geom[i].index;
+            return sh.geom[i];
         };
         // Copies tile i into buffer i % 2 (a cp.async group is closed either way).
         auto prefetch = [&](uint32_t i) {
             if (i < count) {
                 const tsk_encode_image *im;
                 uint64_t index;
-                const TileGeom geom = tile(i, im, index);
-                issue_tile_any(sh, i % 2, *im, geom);
+                const TileGeom &geom = tile(i, im, index);
+                issue_tile_any<AnyF32>(sh, i % 2, *im, geom);
             } else {
                 cp_async_commit();
             }
@@ -502,11 +579,11 @@ __device__ void encode_chunks(EncodeShared &sh, const Images &images, uint64_t t
             __syncthreads();
             const tsk_encode_image *im;
             uint64_t index;
-            const TileGeom geom = tile(i, im, index);
+            const TileGeom &geom = tile(i, im, index);
             const Segment seg = segment_of(geom);
             uint32_t z[kSeg];
-            if (im->type == 2) {
-                analyze_tile<true>(sh, i % 2, geom, seg, z);
+            if (AnyF32 && im->type == 2) {
+                analyze_tile<AnyF32>(sh, i % 2, geom, seg, z);
             } else {
                 analyze_tile<false>(sh, i % 2, geom, seg, z);
             }
@@ -575,13 +652,13 @@ __device__ void encode_chunks(EncodeShared &sh, const Images &images, uint64_t t
             const uint32_t m = sh.image[i];
             const tsk_encode_image *im;
             uint64_t index;
-            const TileGeom geom = tile(i, im, index);
+            const TileGeom &geom = tile(i, im, index);
             const uint64_t offset = 64 + 32 * im->tile_count + sh.offset[i];
             const Segment seg = segment_of(geom);
             uint32_t z[kSeg];
-            if (im->type == 2) {
-                analyze_tile<true>(sh, i % 2, geom, seg, z);
-                write_tile<true>(sh, i % 2, *im, index, geom, seg, z, offset);
+            if (AnyF32 && im->type == 2) {
+                analyze_tile<AnyF32>(sh, i % 2, geom, seg, z);
+                write_tile<AnyF32>(sh, i % 2, *im, index, geom, seg, z, offset);
             } else {
                 analyze_tile<false>(sh, i % 2, geom, seg, z);
                 write_tile<false>(sh, i % 2, *im, index, geom, seg, z, offset);
@@ -598,13 +675,19 @@ __device__ void encode_chunks(EncodeShared &sh, const Images &images, uint64_t t
     }
 }
 
-__global__ void __launch_bounds__(kThreads)
+template <bool AnyF32> using SharedFor = EncodeShared<AnyF32 ? 4096u : 2048u>;
+
+// AnyF32: the batch has FP32 images (16 KiB tile buffers); otherwise 8 KiB buffers and a
+// 40-register bound, so that six CTAs fit on an SM.
+template <bool AnyF32>
+__global__ void __launch_bounds__(kThreads, AnyF32 ? 1 : 6)
     encode_kernel(const tsk_encode_image *__restrict__ images, uint32_t image_count,
                   uint64_t total_tiles, uint32_t chunk_tiles, uint64_t *state,
                   tsk_result *results) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
-    EncodeShared &sh = *reinterpret_cast<EncodeShared *>(smem_raw);
-    encode_chunks(sh, ImageTable{images, image_count}, total_tiles, chunk_tiles, state, results);
+    auto &sh = *reinterpret_cast<SharedFor<AnyF32> *>(smem_raw);
+    encode_chunks<AnyF32>(sh, ImageTable{images, image_count}, total_tiles, chunk_tiles, state,
+                          results);
 }
 
 // Tiles per chunk for a launch of `grid` CTAs: as many as spread the tiles over the grid in one
@@ -623,18 +706,18 @@ extern "C" uint64_t tsk_encode_state_bytes(uint64_t total_tiles) {
 
 extern "C" int tsk_encode_prepare(int device) {
     (void)device;
-    cudaError_t e = cudaFuncSetAttribute(tsk::encode_kernel,
+    cudaError_t e = cudaFuncSetAttribute(tsk::encode_kernel<true>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(sizeof(tsk::EncodeShared)));
+                                         static_cast<int>(sizeof(tsk::SharedFor<true>)));
     if (e != cudaSuccess) return e;
-    cudaFuncAttributes attributes;
-    return cudaFuncGetAttributes(&attributes, tsk::encode_kernel);
+    return cudaFuncSetAttribute(tsk::encode_kernel<false>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(sizeof(tsk::SharedFor<false>)));
 }
 
 extern "C" int tsk_encode_launch(const tsk_encode_image *images, uint32_t image_count,
                                  uint64_t total_tiles, uint32_t any_float, void *state,
                                  tsk_result *results, cudaStream_t stream) {
-    (void)any_float;
     if (total_tiles == 0) return cudaSuccess;
     cudaError_t e = cudaMemsetAsync(state, 0, tsk_encode_state_bytes(total_tiles), stream);
     if (e != cudaSuccess) return e;
@@ -645,15 +728,15 @@ extern "C" int tsk_encode_launch(const tsk_encode_image *images, uint32_t image_
     if (e != cudaSuccess) return e;
     e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     if (e != cudaSuccess) return e;
-    const size_t smem = sizeof(tsk::EncodeShared);
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tsk::encode_kernel, tsk::kThreads,
-                                                      smem);
+    auto kernel = any_float ? tsk::encode_kernel<true> : tsk::encode_kernel<false>;
+    const size_t smem = any_float ? sizeof(tsk::SharedFor<true>) : sizeof(tsk::SharedFor<false>);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, tsk::kThreads, smem);
     if (e != cudaSuccess) return e;
     uint64_t grid = static_cast<uint64_t>(sms) * (per_sm > 0 ? per_sm : 1);
     const uint32_t k = tsk::chunk_tiles_for(total_tiles, grid);
     const uint64_t chunks = (total_tiles + k - 1) / k;
     if (grid > chunks) grid = chunks;
-    tsk::encode_kernel<<<static_cast<uint32_t>(grid), tsk::kThreads, smem, stream>>>(
+    kernel<<<static_cast<uint32_t>(grid), tsk::kThreads, smem, stream>>>(
         images, image_count, total_tiles, k, static_cast<uint64_t *>(state), results);
     return cudaGetLastError();
 }
@@ -681,18 +764,19 @@ constexpr uint64_t kStaticStateWords = 131072;
 
 __device__ __align__(256) uint64_t g_encode_scratch[kStaticStateWords];
 
-__global__ void __launch_bounds__(kThreads)
+template <bool AnyF32>
+__global__ void __launch_bounds__(kThreads, AnyF32 ? 1 : 6)
     encode_kernel_static(const __grid_constant__ tsk_encode_image image, uint64_t total_tiles,
                          uint32_t chunk_tiles, uint64_t *state, tsk_result *result) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
-    EncodeShared &sh = *reinterpret_cast<EncodeShared *>(smem_raw);
-    encode_chunks(sh, SingleImage{&image}, total_tiles, chunk_tiles, state, result);
+    auto &sh = *reinterpret_cast<SharedFor<AnyF32> *>(smem_raw);
+    encode_chunks<AnyF32>(sh, SingleImage{&image}, total_tiles, chunk_tiles, state, result);
 }
 
 // Per-device set-up, done by the first call on each device with that device current.
 struct StaticSetup {
     uint64_t *scratch = nullptr; // device address of g_encode_scratch
-    uint32_t grid = 0;
+    uint32_t grid[2] = {0, 0};   // persistent grids of the uint16 and FP32 instances
 };
 
 constexpr int kMaxDevices = 64;
@@ -708,17 +792,20 @@ cudaError_t static_setup(int device, StaticSetup &out) {
         // the runtime returns this device's copy of the array.
         cudaError_t e = cudaGetSymbolAddress(&address, g_encode_scratch);
         if (e != cudaSuccess) return e;
-        const size_t smem = sizeof(EncodeShared);
-        e = cudaFuncSetAttribute(encode_kernel_static, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(smem));
-        if (e != cudaSuccess) return e;
-        int sms = 0, per_sm = 0;
+        int sms = 0;
         e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
         if (e != cudaSuccess) return e;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, encode_kernel_static, kThreads,
-                                                          smem);
-        if (e != cudaSuccess) return e;
-        s.grid = static_cast<uint32_t>(sms * (per_sm > 0 ? per_sm : 1));
+        for (int f32 = 0; f32 < 2; ++f32) {
+            auto kernel = f32 ? encode_kernel_static<true> : encode_kernel_static<false>;
+            const size_t smem = f32 ? sizeof(SharedFor<true>) : sizeof(SharedFor<false>);
+            e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(smem));
+            if (e != cudaSuccess) return e;
+            int per_sm = 0;
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, smem);
+            if (e != cudaSuccess) return e;
+            s.grid[f32] = static_cast<uint32_t>(sms * (per_sm > 0 ? per_sm : 1));
+        }
         s.scratch = static_cast<uint64_t *>(address);
     }
     out = s;
@@ -750,11 +837,14 @@ extern "C" int tsk_encode_static_launch(const tsk_encode_image *image, tsk_resul
     if (e != cudaSuccess) return e;
     e = cudaMemsetAsync(result, 0, sizeof(tsk_result), stream);
     if (e != cudaSuccess) return e;
-    const uint32_t k = tsk::chunk_tiles_for(total, setup.grid);
+    const bool f32 = image->type == 2;
+    const uint32_t full = setup.grid[f32 ? 1 : 0];
+    const uint32_t k = tsk::chunk_tiles_for(total, full);
     const uint64_t chunks = (total + k - 1) / k;
-    const uint64_t grid = setup.grid < chunks ? setup.grid : chunks;
-    tsk::encode_kernel_static<<<static_cast<uint32_t>(grid), tsk::kThreads,
-                                sizeof(tsk::EncodeShared), stream>>>(*image, total, k,
-                                                                     setup.scratch, result);
+    const uint64_t grid = full < chunks ? full : chunks;
+    auto kernel = f32 ? tsk::encode_kernel_static<true> : tsk::encode_kernel_static<false>;
+    const size_t smem = f32 ? sizeof(tsk::SharedFor<true>) : sizeof(tsk::SharedFor<false>);
+    kernel<<<static_cast<uint32_t>(grid), tsk::kThreads, smem, stream>>>(*image, total, k,
+                                                                         setup.scratch, result);
     return cudaGetLastError();
 }
