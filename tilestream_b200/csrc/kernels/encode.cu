@@ -6,21 +6,24 @@
 // does all of it:
 //
 //  1. a CTA claims the next chunk of k consecutive tiles (in batch order, from an atomic
-//     counter; k = ceil(tiles / grid), at most kMaxChunk) and, tile by tile, loads the pixels
-//     into shared memory and computes the residuals (zigzag mod 2^16 or XOR, encoder.cpp:32-37);
-//     one warp per row OR-reduces them with shuffles, the row width is the index of the highest
-//     set bit (docs/format.md:101), the row costs are scanned with a warp shuffle scan, and the
-//     canonical mode is chosen with the tie order RAW < CONSTANT < PREDICT
-//     (docs/format.md:103-109, encoder.cpp:69-78);
+//     counter; k = ceil(tiles / grid), at most the shared-memory payload slots: 4 uint16 or 2
+//     FP32 tiles) and, tile by tile, copies the pixels into shared memory (16-byte cp.async, the
+//     next tile in flight while the current one is encoded). Each thread takes a 16-sample
+//     segment of a row and computes its residuals in registers (zigzag mod 2^16 or XOR,
+//     encoder.cpp:32-37); the row width is the index of the highest set bit of the row's OR
+//     (docs/format.md:101), the row costs are scanned with a warp shuffle scan, and the canonical
+//     mode is chosen with the tie order RAW < CONSTANT < PREDICT (docs/format.md:103-109,
+//     encoder.cpp:69-78). The tile is then encoded into its payload slot in shared memory: each
+//     thread appends its residuals to the row's bit stream;
 //  2. the chunk publishes the summed lengths of its tiles of its last image; one warp then looks
 //     back over the earlier chunks of its first image, 32 chunks per step, stopping at the
 //     image's first chunk or at a chunk that has published its inclusive prefix. Every chunk
-//     publishes its sum as soon as its own tiles are analysed, so the look-back waits for no
+//     publishes its sum as soon as its own tiles are encoded, so the look-back waits for no
 //     chain of prefixes (a look-back per tile would: tiles are small and many are in flight).
 //     Waits are bounded and report cuda_error instead of hanging;
-//  3. the CTA reloads each tile of the chunk (still in L2), recomputes its residuals and writes
-//     the index entry and every payload word, each word by exactly one thread (encoder.cu:157-173
-//     gathers the same bits from global memory);
+//  3. the CTA writes the index entries and copies the payloads out, each word by exactly one
+//     thread (the reference's pack gathers the same bits from global memory,
+//     encoder.cu:157-173);
 //  4. the last tile of an image writes the 64-byte header and the image's DeviceResult.
 #include "ptx.cuh"
 #include "tasks.h"
@@ -62,11 +65,13 @@ struct TileGeom {
 
 // Words: the largest tile in 32-bit words, 2048 for uint16-only batches (4096 samples) and
 // 4096 when the batch has FP32 images; a PREDICT payload is always shorter than the RAW one.
-template <uint32_t Words> struct EncodeShared {
+// Slots: payloads of a chunk kept until its offsets are known (the most tiles in a chunk).
+template <uint32_t Words, uint32_t Slots> struct EncodeShared {
+    static constexpr uint32_t kSlots = Slots;
     // Two tile buffers: the tile being analysed and the next one in flight. Rows are packed
     // (w samples each), as uint16 or FP32 words.
     alignas(16) uint32_t raw[2][Words];
-    uint32_t stage[Words]; // the tile payload being written (PREDICT)
+    alignas(16) uint32_t payload[Slots][Words]; // the chunk's encoded payloads
     uint32_t row_or[TSK_MAX_ROWS];         // OR of each row's residuals
     uint32_t bits[TSK_MAX_ROWS];
     uint32_t row_word[TSK_MAX_ROWS + 1]; // first payload word of each row
@@ -78,6 +83,7 @@ template <uint32_t Words> struct EncodeShared {
     uint32_t count;
     uint32_t image[kMaxChunk];  // image of each tile of the chunk
     TileGeom geom[kMaxChunk];
+    uint32_t mode_of[kMaxChunk];
     uint32_t length_of[kMaxChunk];
     uint64_t offset[kMaxChunk]; // payload offset of each tile within its image's payload area
 };
@@ -241,7 +247,7 @@ __device__ __forceinline__ void segment_residuals(const Sh &sh, uint32_t buf,
 }
 
 // Row widths, the constant test, the row-cost scan and the canonical mode; sets sh.bits,
-// sh.row_word, sh.mode and sh.length. z keeps the segment's residuals for write_tile.
+// sh.row_word, sh.mode and sh.length. z keeps the segment's residuals for pack_tile.
 template <bool F32, typename Sh>
 __device__ void analyze_tile(Sh &sh, uint32_t buf, const TileGeom &g,
                              const Segment &seg, uint32_t (&z)[kSeg]) {
@@ -304,57 +310,38 @@ __device__ void analyze_tile(Sh &sh, uint32_t buf, const TileGeom &g,
     __syncthreads();
 }
 
-// Index entry and payload of an analysed tile, one writer per word; `offset` is the payload's
-// absolute position in the file. PREDICT rows are packed in shared memory first: each thread
-// appends its segment's residuals to the row's bit stream (docs/format.md:77) through a 64-bit
-// accumulator, OR-ing the words it touches, and the CTA then copies the payload out.
+// Encodes an analysed tile into payload slot `slot`. PREDICT rows: each thread appends its
+// segment's residuals to the row's bit stream (docs/format.md:77) through a 64-bit accumulator,
+// OR-ing the words it touches into the slot (cleared before the tile's first barrier). RAW: the
+// tile buffer holds the rows packed, so it is copied, zero-padded to a word. CONSTANT: one word.
 template <bool F32, typename Sh>
-__device__ void write_tile(Sh &sh, uint32_t buf, const tsk_encode_image &im,
-                           uint64_t index, const TileGeom &g, const Segment &seg,
-                           const uint32_t (&z)[kSeg], uint64_t offset) {
+__device__ void pack_tile(Sh &sh, uint32_t buf, uint32_t slot, const TileGeom &g,
+                          const Segment &seg, const uint32_t (&z)[kSeg]) {
     const uint32_t w = g.w, h = g.h;
-    uint8_t *file = reinterpret_cast<uint8_t *>(im.output);
-    const uint32_t mode = sh.mode, length = sh.length;
-    const uint32_t words = length / 4;
-    if (threadIdx.x < 8) {
-        uint32_t v = 0;
-        switch (threadIdx.x) {
-        case 0: v = mode; break;
-        case 1: v = w | (h << 16); break;
-        case 2: v = static_cast<uint32_t>(offset); break;
-        case 3: v = static_cast<uint32_t>(offset >> 32); break;
-        case 4: v = length; break;
-        default: v = 0; break;
-        }
-        put_word(file, 64 + 32 * index + 4 * threadIdx.x, v);
-    }
+    const uint32_t mode = sh.mode, words = sh.length / 4;
+    uint32_t *out = sh.payload[slot];
     if (mode == TSK_RAW) {
-        // The tile buffer holds the rows packed: it is the payload, zero-padded to a word.
         const uint32_t bytes = w * h * (F32 ? 4 : 2);
         for (uint32_t k = threadIdx.x; k < words; k += kThreads) {
             uint32_t v = sh.raw[buf][k];
             if (4 * k + 4 > bytes) {
                 v &= 0xffffu; // an odd number of uint16 samples
             }
-            put_word(file, offset + 4ull * k, v);
+            out[k] = v;
         }
         return;
     }
     if (mode == TSK_CONSTANT) {
         if (threadIdx.x == 0) {
-            put_word(file, offset, px<F32>(sh, buf, 0));
+            out[0] = px<F32>(sh, buf, 0);
         }
         return;
     }
-    for (uint32_t k = threadIdx.x; k < words; k += kThreads) {
-        sh.stage[k] = 0;
-    }
-    __syncthreads();
     if (seg.n != 0) {
         const uint32_t r = seg.r, b = sh.bits[r], row = sh.row_word[r];
         if (seg.c0 == 0) {
-            sh.stage[row] = px<F32>(sh, buf, r * w); // seed
-            sh.stage[row + 1] = b;                   // width word; reserved bytes zero
+            out[row] = px<F32>(sh, buf, r * w); // seed
+            out[row + 1] = b;                   // width word; reserved bytes zero
         }
         if (b != 0) {
             // Residual j (column j + 1) starts at bit j * b of the row's packed words.
@@ -368,7 +355,7 @@ __device__ void write_tile(Sh &sh, uint32_t buf, const tsk_encode_image &im,
                 acc |= static_cast<uint64_t>(v) << bit;
                 bit += bits;
                 if (bit >= 32) {
-                    atomicOr(&sh.stage[at], static_cast<uint32_t>(acc));
+                    atomicOr(&out[at], static_cast<uint32_t>(acc));
                     acc >>= 32;
                     bit -= 32;
                     ++at;
@@ -398,13 +385,34 @@ __device__ void write_tile(Sh &sh, uint32_t buf, const tsk_encode_image &im,
                 }
             }
             if (bit != 0) {
-                atomicOr(&sh.stage[at], static_cast<uint32_t>(acc));
+                atomicOr(&out[at], static_cast<uint32_t>(acc));
             }
         }
     }
-    __syncthreads();
-    for (uint32_t k = threadIdx.x; k < words; k += kThreads) {
-        put_word(file, offset + 4ull * k, sh.stage[k]);
+}
+
+// Index entry of a tile and its payload copied from its slot into the file at `offset` (the
+// payload's absolute position), one writer per word.
+template <typename Sh>
+__device__ void store_tile(const Sh &sh, uint32_t slot, const tsk_encode_image &im,
+                           uint64_t index, const TileGeom &g, uint32_t mode, uint32_t length,
+                           uint64_t offset) {
+    uint8_t *file = reinterpret_cast<uint8_t *>(im.output);
+    if (threadIdx.x < 8) {
+        uint32_t v = 0;
+        switch (threadIdx.x) {
+        case 0: v = mode; break;
+        case 1: v = g.w | (g.h << 16); break;
+        case 2: v = static_cast<uint32_t>(offset); break;
+        case 3: v = static_cast<uint32_t>(offset >> 32); break;
+        case 4: v = length; break;
+        default: v = 0; break;
+        }
+        put_word(file, 64 + 32 * index + 4 * threadIdx.x, v);
+    }
+    const uint32_t *in = sh.payload[slot];
+    for (uint32_t k = threadIdx.x; k < length / 4; k += kThreads) {
+        put_word(file, offset + 4ull * k, in[k]);
     }
 }
 
@@ -571,12 +579,17 @@ __device__ void encode_chunks(Sh &sh, const Images &images, uint64_t total_tiles
             }
         };
 
-        // 1. Lengths of the chunk's tiles; tile i + 1 is copied while tile i is analysed.
+        // 1. Encode the chunk's tiles into their payload slots; tile i + 1 is copied while tile i
+        //    is encoded.
         prefetch(0);
         for (uint32_t i = 0; i < count; ++i) {
-            prefetch(i + 1);
-            cp_async_wait<1>();
+            for (uint32_t k = threadIdx.x; k < sizeof(sh.payload[0]) / 16; k += kThreads) {
+                reinterpret_cast<uint4 *>(sh.payload[i])[k] = make_uint4(0, 0, 0, 0);
+            }
+            cp_async_wait<0>();
+            // Tile i has landed, and every thread is done with tile i - 1 (its buffer is free).
             __syncthreads();
+            prefetch(i + 1);
             const tsk_encode_image *im;
             uint64_t index;
             const TileGeom &geom = tile(i, im, index);
@@ -584,18 +597,20 @@ __device__ void encode_chunks(Sh &sh, const Images &images, uint64_t total_tiles
             uint32_t z[kSeg];
             if (AnyF32 && im->type == 2) {
                 analyze_tile<AnyF32>(sh, i % 2, geom, seg, z);
+                pack_tile<AnyF32>(sh, i % 2, i, geom, seg, z);
             } else {
                 analyze_tile<false>(sh, i % 2, geom, seg, z);
+                pack_tile<false>(sh, i % 2, i, geom, seg, z);
             }
             if (threadIdx.x == 0) {
+                sh.mode_of[i] = sh.mode;
                 sh.length_of[i] = sh.length;
             }
             if (threadIdx.x < TSK_MAX_ROWS) {
                 sh.row_or[threadIdx.x] = 0; // for the next tile (read before the last barrier)
             }
         }
-        // The first tile's copy for step 3 flies during the look-back.
-        prefetch(0);
+        cp_async_wait<0>();
         __syncthreads();
 
         // 2. Offsets: within the chunk, then the carry of the first image from earlier chunks.
@@ -646,41 +661,27 @@ __device__ void encode_chunks(Sh &sh, const Images &images, uint64_t total_tiles
 
         // 3. Index entries and payloads; the last tile of an image writes its header.
         for (uint32_t i = 0; i < count; ++i) {
-            prefetch(i + 1);
-            cp_async_wait<1>();
-            __syncthreads();
             const uint32_t m = sh.image[i];
             const tsk_encode_image *im;
             uint64_t index;
             const TileGeom &geom = tile(i, im, index);
             const uint64_t offset = 64 + 32 * im->tile_count + sh.offset[i];
-            const Segment seg = segment_of(geom);
-            uint32_t z[kSeg];
-            if (AnyF32 && im->type == 2) {
-                analyze_tile<AnyF32>(sh, i % 2, geom, seg, z);
-                write_tile<AnyF32>(sh, i % 2, *im, index, geom, seg, z, offset);
-            } else {
-                analyze_tile<false>(sh, i % 2, geom, seg, z);
-                write_tile<false>(sh, i % 2, *im, index, geom, seg, z, offset);
-            }
-            if (threadIdx.x < TSK_MAX_ROWS) {
-                sh.row_or[threadIdx.x] = 0; // for the next tile (read before the last barrier)
-            }
+            store_tile(sh, i, *im, index, geom, sh.mode_of[i], sh.length_of[i], offset);
             if (index + 1 == im->tile_count) {
                 write_header(*im, sh.offset[i] + sh.length_of[i], results + m);
             }
-            __syncthreads();
         }
-        cp_async_wait<0>();
+        __syncthreads();
     }
 }
 
-template <bool AnyF32> using SharedFor = EncodeShared<AnyF32 ? 4096u : 2048u>;
+// AnyF32: the batch has FP32 images (16 KiB tile buffers and payload slots, two tiles per
+// chunk: 64 KiB); otherwise 8 KiB buffers and slots, four tiles per chunk (48 KiB), four CTAs
+// per SM.
+template <bool AnyF32> using SharedFor = EncodeShared<AnyF32 ? 4096u : 2048u, AnyF32 ? 2u : 4u>;
 
-// AnyF32: the batch has FP32 images (16 KiB tile buffers); otherwise 8 KiB buffers and a
-// 40-register bound, so that six CTAs fit on an SM.
 template <bool AnyF32>
-__global__ void __launch_bounds__(kThreads, AnyF32 ? 1 : 6)
+__global__ void __launch_bounds__(kThreads, AnyF32 ? 1 : 4)
     encode_kernel(const tsk_encode_image *__restrict__ images, uint32_t image_count,
                   uint64_t total_tiles, uint32_t chunk_tiles, uint64_t *state,
                   tsk_result *results) {
@@ -691,10 +692,11 @@ __global__ void __launch_bounds__(kThreads, AnyF32 ? 1 : 6)
 }
 
 // Tiles per chunk for a launch of `grid` CTAs: as many as spread the tiles over the grid in one
-// round, at most kMaxChunk (larger batches take several rounds).
-uint32_t chunk_tiles_for(uint64_t total_tiles, uint64_t grid) {
+// round, at most the instance's payload slots (larger batches take several rounds).
+uint32_t chunk_tiles_for(uint64_t total_tiles, uint64_t grid, bool any_f32) {
+    const uint64_t most = any_f32 ? SharedFor<true>::kSlots : SharedFor<false>::kSlots;
     const uint64_t k = (total_tiles + grid - 1) / grid;
-    return static_cast<uint32_t>(k < 1 ? 1 : (k > kMaxChunk ? kMaxChunk : k));
+    return static_cast<uint32_t>(k < 1 ? 1 : (k > most ? most : k));
 }
 
 } // namespace
@@ -733,7 +735,7 @@ extern "C" int tsk_encode_launch(const tsk_encode_image *images, uint32_t image_
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, tsk::kThreads, smem);
     if (e != cudaSuccess) return e;
     uint64_t grid = static_cast<uint64_t>(sms) * (per_sm > 0 ? per_sm : 1);
-    const uint32_t k = tsk::chunk_tiles_for(total_tiles, grid);
+    const uint32_t k = tsk::chunk_tiles_for(total_tiles, grid, any_float != 0);
     const uint64_t chunks = (total_tiles + k - 1) / k;
     if (grid > chunks) grid = chunks;
     kernel<<<static_cast<uint32_t>(grid), tsk::kThreads, smem, stream>>>(
@@ -765,7 +767,7 @@ constexpr uint64_t kStaticStateWords = 131072;
 __device__ __align__(256) uint64_t g_encode_scratch[kStaticStateWords];
 
 template <bool AnyF32>
-__global__ void __launch_bounds__(kThreads, AnyF32 ? 1 : 6)
+__global__ void __launch_bounds__(kThreads, AnyF32 ? 1 : 4)
     encode_kernel_static(const __grid_constant__ tsk_encode_image image, uint64_t total_tiles,
                          uint32_t chunk_tiles, uint64_t *state, tsk_result *result) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
@@ -839,7 +841,7 @@ extern "C" int tsk_encode_static_launch(const tsk_encode_image *image, tsk_resul
     if (e != cudaSuccess) return e;
     const bool f32 = image->type == 2;
     const uint32_t full = setup.grid[f32 ? 1 : 0];
-    const uint32_t k = tsk::chunk_tiles_for(total, full);
+    const uint32_t k = tsk::chunk_tiles_for(total, full, f32);
     const uint64_t chunks = (total + k - 1) / k;
     const uint64_t grid = full < chunks ? full : chunks;
     auto kernel = f32 ? tsk::encode_kernel_static<true> : tsk::encode_kernel_static<false>;
