@@ -439,7 +439,8 @@ def run_reference(args):
     seconds = sum(e for _, e in per_step)
     value = images * W * H * 2 / seconds / 1e9
     return {
-        "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": 0,
+        "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": args.gpus,
+        "device": "host CPU cores (the reference codec has no GPU path to call here)",
         "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(seconds / len(per_step) * 1e3, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u16", "impl": "reference",
