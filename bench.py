@@ -790,7 +790,7 @@ def run_serving(args, torch, stream):
     serial_count = min(len(requests), args.serve_serial_requests)
     serial_requests = (cuda.N.ServeRequest * serial_count)(*requests[:serial_count])
     warm = workloads.serving_requests(200, n, side, side, rate, seed=6)
-    results = {}
+    results, servers = {}, {}
     for name, options, reqs in (
             ("continuous_batching", dict(max_batch=48, max_inflight=4), requests),
             ("one_at_a_time_resident", dict(max_batch=1, max_inflight=1), requests),
@@ -806,7 +806,22 @@ def run_serving(args, torch, stream):
         assert st == Status.success, st
         ok = all(outcomes[i].result.status == 0 for i in range(len(reqs)))
         results[name] = {**serve_summary(stats, len(reqs)), "all_success": ok}
-        del srv
+        servers[name] = srv
+    # Offered rate sweep (same request distribution, 10,000 requests per point): where
+    # continuous batching and one request at a time part.
+    sweep = []
+    for r in args.serve_sweep:
+        arrays = workloads.serving_requests(10000, n, side, side, r, seed=7)
+        point = {"offered_rps": r}
+        for name in ("continuous_batching", "one_at_a_time_resident"):
+            st, outcomes, stats = servers[name].run(cuda.serve_requests(arrays))
+            assert st == Status.success, st
+            point[name] = {k: v for k, v in serve_summary(stats, 10000).items()
+                           if k in ("p50_ms", "p99_ms", "throughput_rps", "decoded_gbs",
+                                    "mean_batch", "max_inflight", "stalls")}
+        sweep.append(point)
+    results["rate_sweep"] = sweep
+    servers.clear()
     area = stream_arrays["width"].astype(np.float64) * stream_arrays["height"]
     return {"workload": f"{n} uint16 {side}x{side} archives, 64x64 tiles, resident; Poisson "
                         f"arrivals at {rate:.0f} req/s; ROI sides log-uniform 32..4096 at a "
@@ -901,6 +916,9 @@ def main():
                    help="requests of the one-at-a-time plan-API baseline")
     p.add_argument("--serve-rate", type=float, default=20000.0, help="offered requests/s")
     p.add_argument("--serve-pool-gb", type=int, default=2)
+    p.add_argument("--serve-sweep", type=lambda v: [float(x) for x in v.split(",") if x],
+                   default=[50000.0, 100000.0, 200000.0, 400000.0],
+                   help="offered rates (req/s) of the serving sweep")
     args = p.parse_args()
     args.warmup = max(args.warmup, 3)
 

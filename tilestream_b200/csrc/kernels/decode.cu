@@ -948,6 +948,10 @@ Variant select(uint32_t paths, uint32_t shape) {
         if (c && !plain) {
             return narrow ? make<16384, 3, kF32 | kCal, 4, 16, 4>() : make<16384, 3, kF32 | kCal>();
         }
+    } else if (plain && !c) {
+        // Mixed uint16 and FP32 archives, plain decode (no calibrated code in the instance).
+        return narrow ? make<16384, 3, kU16 | kF32 | kPlain, 4, 16, 4>()
+                      : make<16384, 3, kU16 | kF32 | kPlain>();
     }
     return narrow ? make<16384, 3, kU16 | kF32 | kPlain | kCal, 4, 16, 4>()
                   : make<16384, 3, kU16 | kF32 | kPlain | kCal>();
