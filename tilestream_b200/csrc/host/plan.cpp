@@ -286,7 +286,9 @@ Status draft_calibrate(const BatchRequest &request, Draft &d) {
         c.type = static_cast<std::uint32_t>(item.input.image.type);
         const auto image = static_cast<std::uint32_t>(d.calib_images.size());
         // Chunks of about 16 Ki pixels keep every SM streaming on small and large images alike.
-        const std::uint32_t chunk = std::max<std::uint32_t>(1, 16384 / c.width);
+        // About 4 Ki pixels per task: enough work per task, and rounds fine enough that the
+        // persistent grid ends evenly.
+        const std::uint32_t chunk = std::max<std::uint32_t>(1, 4096 / c.width);
         for (std::uint32_t y = 0; y < c.height; y += chunk) {
             tsk_calib_task t{};
             t.image = image;

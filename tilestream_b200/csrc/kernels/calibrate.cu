@@ -48,25 +48,46 @@ __device__ void calibrate_rows(const tsk_calib_image &im, uint32_t y0, uint32_t 
         uint32_t x = 0;
         if (misalign == 0) {
             const uint32_t vec_end = width & ~3u;
-            for (x = threadIdx.x * 4; x < vec_end; x += kThreads * 4) {
+            constexpr uint32_t kStep = kThreads * 4;
+            // Groups of four samples; two groups per iteration, all their loads issued before
+            // any result is computed.
+            struct Group {
                 uint32_t v[4];
+                float4 o, g;
+            };
+            auto load = [&](uint32_t at, Group &q) {
                 if constexpr (F32) {
-                    const uint4 q = __ldg(reinterpret_cast<const uint4 *>(in + 4ull * x));
-                    v[0] = q.x, v[1] = q.y, v[2] = q.z, v[3] = q.w;
+                    const uint4 w = __ldg(reinterpret_cast<const uint4 *>(in + 4ull * at));
+                    q.v[0] = w.x, q.v[1] = w.y, q.v[2] = w.z, q.v[3] = w.w;
                 } else {
-                    const uint2 q = __ldg(reinterpret_cast<const uint2 *>(in + 2ull * x));
-                    v[0] = q.x & 0xffffu, v[1] = q.x >> 16, v[2] = q.y & 0xffffu, v[3] = q.y >> 16;
+                    const uint2 w = __ldg(reinterpret_cast<const uint2 *>(in + 2ull * at));
+                    q.v[0] = w.x & 0xffffu, q.v[1] = w.x >> 16;
+                    q.v[2] = w.y & 0xffffu, q.v[3] = w.y >> 16;
                 }
-                float4 o = make_float4(im.offset, im.offset, im.offset, im.offset);
-                float4 g = make_float4(im.gain, im.gain, im.gain, im.gain);
-                if (om) o = __ldg(reinterpret_cast<const float4 *>(om + x));
-                if (gm) g = __ldg(reinterpret_cast<const float4 *>(gm + x));
+                q.o = om ? __ldg(reinterpret_cast<const float4 *>(om + at))
+                         : make_float4(im.offset, im.offset, im.offset, im.offset);
+                q.g = gm ? __ldg(reinterpret_cast<const float4 *>(gm + at))
+                         : make_float4(im.gain, im.gain, im.gain, im.gain);
+            };
+            auto store = [&](uint32_t at, const Group &q) {
                 float4 r;
-                r.x = cal(to_float<F32>(v[0]), o.x, g.x);
-                r.y = cal(to_float<F32>(v[1]), o.y, g.y);
-                r.z = cal(to_float<F32>(v[2]), o.z, g.z);
-                r.w = cal(to_float<F32>(v[3]), o.w, g.w);
-                __stcs(reinterpret_cast<float4 *>(out + x), r);
+                r.x = cal(to_float<F32>(q.v[0]), q.o.x, q.g.x);
+                r.y = cal(to_float<F32>(q.v[1]), q.o.y, q.g.y);
+                r.z = cal(to_float<F32>(q.v[2]), q.o.z, q.g.z);
+                r.w = cal(to_float<F32>(q.v[3]), q.o.w, q.g.w);
+                __stcs(reinterpret_cast<float4 *>(out + at), r);
+            };
+            for (x = threadIdx.x * 4; x + kStep < vec_end; x += 2 * kStep) {
+                Group a, b;
+                load(x, a);
+                load(x + kStep, b);
+                store(x, a);
+                store(x + kStep, b);
+            }
+            if (x < vec_end) {
+                Group a;
+                load(x, a);
+                store(x, a);
             }
             x = vec_end + threadIdx.x;
         } else {
