@@ -15,11 +15,13 @@
 //     mode is chosen with the tie order RAW < CONSTANT < PREDICT (docs/format.md:103-109,
 //     encoder.cpp:69-78). The tile is then encoded into its payload slot in shared memory: each
 //     thread appends its residuals to the row's bit stream;
-//  2. the chunk publishes the summed lengths of its tiles of its last image; one warp then looks
-//     back over the earlier chunks of its first image, 32 chunks per step, stopping at the
-//     image's first chunk or at a chunk that has published its inclusive prefix. Every chunk
-//     publishes its sum as soon as its own tiles are encoded, so the look-back waits for no
-//     chain of prefixes (a look-back per tile would: tiles are small and many are in flight).
+//  2. the chunk publishes the summed lengths of its tiles of its last image, in its own word and
+//     added (with an arrival count) to the word of its group of 32 chunks. One warp then sums
+//     the earlier chunks of its first image: whole groups from their group words, the chunks
+//     at either end from their own words, up to 128 words per step with every load in flight
+//     at once. Each word read is final as soon as the chunks it covers are analysed, so a
+//     look-back never waits for another look-back (a chain of inclusive prefixes advances one
+//     window per L2 round trip; a look-back per tile would wait on many more chunks).
 //     Waits are bounded and report cuda_error instead of hanging;
 //  3. the CTA writes the index entries and copies the payloads out, each word by exactly one
 //     thread (the reference's pack gathers the same bits from global memory,
@@ -35,9 +37,13 @@ namespace tsk {
 namespace {
 
 constexpr uint32_t kThreads = 256;
-constexpr uint64_t kAggregate = 1ull << 62;
-constexpr uint64_t kPrefix = 2ull << 62;
+// A chunk's word: kPublished | the summed lengths. A group's word: the number of its chunks that
+// have added their lengths, in the top byte, and the sum of those lengths.
+constexpr uint64_t kPublished = 1ull << 62;
 constexpr uint64_t kValue = (1ull << 62) - 1;
+constexpr uint32_t kGroupChunks = 32;
+constexpr uint64_t kGroupArrival = 1ull << 56;
+constexpr uint64_t kGroupValue = kGroupArrival - 1;
 
 constexpr uint32_t kMaxChunk = 8;
 
@@ -491,38 +497,59 @@ struct SingleImage {
     }
 };
 
-// Looks back over chunks [stop, g) (all of them inside one image) from chunk g - 1 downwards,
-// 32 per step, and returns the summed lengths up to the nearest inclusive prefix. Warp 0 only.
-__device__ uint64_t look_back(const uint64_t *flags, uint64_t g, uint64_t stop, bool &timed_out) {
+// Sums the lengths published by chunks [stop, g), warp 0 only. Whole groups inside the range
+// are read from their group words, the chunks before the first whole group and after the last
+// one from their own words: the words are numbered 0 .. n-1 in that order and each lane loads
+// up to kPerLane of every 32 * kPerLane before it waits on any.
+__device__ uint64_t look_back(const uint64_t *flags, const uint64_t *groups, uint64_t g,
+                              uint64_t stop, bool &timed_out) {
+    constexpr uint32_t kPerLane = 4;
     const uint32_t lane = threadIdx.x % 32;
-    uint64_t carry = 0;
-    int64_t j = static_cast<int64_t>(g) - 1;
-    for (;;) {
-        const int64_t idx = j - lane;
-        uint64_t v = kPrefix; // chunks before the image's first one end the walk with nothing
-        if (idx >= static_cast<int64_t>(stop)) {
-            v = ld_acquire(flags + idx);
+    const uint64_t lo = (stop + kGroupChunks - 1) / kGroupChunks, hi = g / kGroupChunks;
+    const bool whole = lo < hi;
+    const uint64_t head = whole ? lo * kGroupChunks - stop : g - stop; // chunks from stop
+    const uint64_t mid = whole ? hi - lo : 0;                          // groups from lo
+    const uint64_t tail_first = whole ? hi * kGroupChunks : g;          // chunks to g
+    const uint64_t n = head + mid + (g - tail_first);
+    auto word = [&](uint64_t i) -> const uint64_t * {
+        return i < head        ? flags + stop + i
+               : i < head + mid ? groups + lo + (i - head)
+                                : flags + tail_first + (i - head - mid);
+    };
+    uint64_t sum = 0;
+    bool late = false;
+    for (uint64_t base = 0; base < n; base += 32 * kPerLane) {
+        uint64_t v[kPerLane];
+#pragma unroll
+        for (uint32_t k = 0; k < kPerLane; ++k) {
+            const uint64_t i = base + k * 32 + lane;
+            v[k] = i < n ? ld_acquire(word(i)) : 0;
+        }
+#pragma unroll
+        for (uint32_t k = 0; k < kPerLane; ++k) {
+            const uint64_t i = base + k * 32 + lane;
+            if (i >= n) {
+                continue;
+            }
+            const bool group = i >= head && i < head + mid;
+            auto ready = [&](uint64_t w) {
+                return group ? (w >> 56) == kGroupChunks : (w >> 62) != 0;
+            };
             uint32_t spins = 0;
-            while ((v >> 62) == 0 && spins < (1u << 22)) {
+            while (!ready(v[k]) && spins < (1u << 22)) {
                 __nanosleep(64);
-                v = ld_acquire(flags + idx);
+                v[k] = ld_acquire(word(i));
                 ++spins;
             }
-            if ((v >> 62) == 0) {
-                timed_out = true;
-                v = kPrefix;
+            if (!ready(v[k])) {
+                late = true;
+            } else {
+                sum += group ? (v[k] & kGroupValue) : (v[k] & kValue);
             }
         }
-        const uint32_t prefixes = __ballot_sync(0xffffffffu, (v >> 62) == 2);
-        const uint32_t upto = prefixes != 0 ? __ffs(prefixes) - 1 : 31u;
-        carry += warp_sum64(lane <= upto ? (v & kValue) : 0ull);
-        if (prefixes != 0) {
-            break;
-        }
-        j -= 32;
     }
-    timed_out = __any_sync(0xffffffffu, timed_out);
-    return carry;
+    timed_out = __any_sync(0xffffffffu, late);
+    return warp_sum64(sum);
 }
 
 // The persistent loop: claim a chunk, analyse its tiles, publish, look back, write.
@@ -531,6 +558,7 @@ __device__ void encode_chunks(Sh &sh, const Images &images, uint64_t total_tiles
                               uint32_t chunk_tiles, uint64_t *state, tsk_result *results) {
     uint64_t *counter = state;
     uint64_t *flags = state + 2;
+    uint64_t *groups = flags + (total_tiles + chunk_tiles - 1) / chunk_tiles;
     const uint32_t warp = threadIdx.x / 32;
     for (;;) {
         if (threadIdx.x == 0) {
@@ -616,7 +644,7 @@ __device__ void encode_chunks(Sh &sh, const Images &images, uint64_t total_tiles
         // 2. Offsets: within the chunk, then the carry of the first image from earlier chunks.
         if (warp == 0) {
             const uint32_t lane = threadIdx.x % 32;
-            const uint32_t first_image = sh.image[0], last_image = sh.image[count - 1];
+            const uint32_t first_image = sh.image[0];
             uint64_t tail = 0; // lengths of the last image's tiles in this chunk
             if (lane == 0) {
                 uint64_t run = 0;
@@ -632,24 +660,17 @@ __device__ void encode_chunks(Sh &sh, const Images &images, uint64_t total_tiles
             __syncwarp();
             tail = __shfl_sync(0xffffffffu, tail, 0);
             const uint64_t image_first = images[first_image].first_tile;
-            const bool carried = image_first < first; // the first image began in an earlier chunk
             if (lane == 0) {
-                // The last image's inclusive prefix at the end of this chunk is already known
-                // unless it is the first image and that began earlier: then only its sum is.
-                const bool known = !carried || first_image != last_image;
-                st_release(flags + g, (known ? kPrefix : kAggregate) | tail);
+                st_release(flags + g, kPublished | tail);
+                atomicAdd(reinterpret_cast<unsigned long long *>(groups + g / kGroupChunks),
+                          static_cast<unsigned long long>(kGroupArrival | tail));
             }
             uint64_t carry = 0;
-            if (carried) {
+            if (image_first < first) { // the first image began in an earlier chunk
                 bool timed_out = false;
-                carry = look_back(flags, g, image_first / chunk_tiles, timed_out);
-                if (lane == 0) {
-                    if (first_image == last_image) {
-                        st_release(flags + g, kPrefix | (carry + tail));
-                    }
-                    if (timed_out) {
-                        atomicCAS(&results[first_image].status, 0u, 9u);
-                    }
+                carry = look_back(flags, groups, g, image_first / chunk_tiles, timed_out);
+                if (lane == 0 && timed_out) {
+                    atomicCAS(&results[first_image].status, 0u, 9u);
                 }
             }
             __syncwarp();
@@ -699,11 +720,17 @@ uint32_t chunk_tiles_for(uint64_t total_tiles, uint64_t grid, bool any_f32) {
     return static_cast<uint32_t>(k < 1 ? 1 : (k > most ? most : k));
 }
 
+// Words of state for a launch of `chunks` chunks: the chunk counter, a spare word, one word per
+// chunk and one per group of chunks.
+uint64_t state_words(uint64_t chunks) {
+    return 2 + chunks + (chunks + kGroupChunks - 1) / kGroupChunks;
+}
+
 } // namespace
 } // namespace tsk
 
 extern "C" uint64_t tsk_encode_state_bytes(uint64_t total_tiles) {
-    return 8 * (total_tiles + 2); // the chunk counter, a spare word, one flag per chunk at most
+    return 8 * tsk::state_words(total_tiles); // a chunk holds one tile at least
 }
 
 extern "C" int tsk_encode_prepare(int device) {
@@ -721,9 +748,7 @@ extern "C" int tsk_encode_launch(const tsk_encode_image *images, uint32_t image_
                                  uint64_t total_tiles, uint32_t any_float, void *state,
                                  tsk_result *results, cudaStream_t stream) {
     if (total_tiles == 0) return cudaSuccess;
-    cudaError_t e = cudaMemsetAsync(state, 0, tsk_encode_state_bytes(total_tiles), stream);
-    if (e != cudaSuccess) return e;
-    e = cudaMemsetAsync(results, 0, sizeof(tsk_result) * image_count, stream);
+    cudaError_t e = cudaMemsetAsync(results, 0, sizeof(tsk_result) * image_count, stream);
     if (e != cudaSuccess) return e;
     int device = 0, sms = 0, per_sm = 0;
     e = cudaGetDevice(&device);
@@ -738,6 +763,8 @@ extern "C" int tsk_encode_launch(const tsk_encode_image *images, uint32_t image_
     const uint32_t k = tsk::chunk_tiles_for(total_tiles, grid, any_float != 0);
     const uint64_t chunks = (total_tiles + k - 1) / k;
     if (grid > chunks) grid = chunks;
+    e = cudaMemsetAsync(state, 0, 8 * tsk::state_words(chunks), stream);
+    if (e != cudaSuccess) return e;
     kernel<<<static_cast<uint32_t>(grid), tsk::kThreads, smem, stream>>>(
         images, image_count, total_tiles, k, static_cast<uint64_t *>(state), results);
     return cudaGetLastError();
@@ -761,7 +788,9 @@ extern "C" int tsk_encode_launch(const tsk_encode_image *images, uint32_t image_
 namespace tsk {
 namespace {
 
-// At most this many tiles per image: 8 bytes of state per tile plus two words, 1 MiB in all.
+// 1 MiB of state: two words, one per chunk and one per 32 chunks. An image with more tiles than
+// the grid has CTAs takes two tiles per chunk at least, so the largest accepted one (131,070
+// tiles) needs at most 67,585 words; an image with fewer tiles than CTAs has a chunk per tile.
 constexpr uint64_t kStaticStateWords = 131072;
 
 __device__ __align__(256) uint64_t g_encode_scratch[kStaticStateWords];
@@ -834,16 +863,18 @@ extern "C" int tsk_encode_static_launch(const tsk_encode_image *image, tsk_resul
     tsk::StaticSetup setup;
     e = tsk::static_setup(device, setup);
     if (e != cudaSuccess) return e;
-    // The array keeps the previous call's contents: clear the counter and this call's flags.
-    e = cudaMemsetAsync(setup.scratch, 0, tsk_encode_state_bytes(total), stream);
-    if (e != cudaSuccess) return e;
-    e = cudaMemsetAsync(result, 0, sizeof(tsk_result), stream);
-    if (e != cudaSuccess) return e;
     const bool f32 = image->type == 2;
     const uint32_t full = setup.grid[f32 ? 1 : 0];
     const uint32_t k = tsk::chunk_tiles_for(total, full, f32);
     const uint64_t chunks = (total + k - 1) / k;
     const uint64_t grid = full < chunks ? full : chunks;
+    const uint64_t words = tsk::state_words(chunks);
+    if (words > tsk::kStaticStateWords) return cudaErrorInvalidValue;
+    // The array keeps the previous call's contents: clear the counter and this call's words.
+    e = cudaMemsetAsync(setup.scratch, 0, 8 * words, stream);
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(result, 0, sizeof(tsk_result), stream);
+    if (e != cudaSuccess) return e;
     auto kernel = f32 ? tsk::encode_kernel_static<true> : tsk::encode_kernel_static<false>;
     const size_t smem = f32 ? sizeof(tsk::SharedFor<true>) : sizeof(tsk::SharedFor<false>);
     kernel<<<static_cast<uint32_t>(grid), tsk::kThreads, smem, stream>>>(*image, total, k,

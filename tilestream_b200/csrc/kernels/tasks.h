@@ -208,8 +208,8 @@ int tsk_serve_launch(const tsk_serve_batch *batch, const tsk_serve_archive *arch
 // Loads the serving kernel instance and returns its persistent grid (SMs x resident CTAs).
 int tsk_serve_prepare(int all_u16, int device, uint32_t *grid);
 
-// Encodes every tile of every image in one pass. state: 8 * (total_tiles + 2) bytes of
-// workspace, cleared by the launcher in stream order.
+// Encodes every tile of every image in one pass. state: tsk_encode_state_bytes(total_tiles)
+// bytes of workspace, cleared by the launcher in stream order.
 int tsk_encode_launch(const tsk_encode_image *images, uint32_t image_count, uint64_t total_tiles,
                       uint32_t any_float, void *state, tsk_result *results, cudaStream_t stream);
 int tsk_encode_prepare(int device);
