@@ -350,11 +350,14 @@ __device__ void pack_tile(Sh &sh, uint32_t buf, uint32_t slot, const TileGeom &g
             out[row + 1] = b;                   // width word; reserved bytes zero
         }
         if (b != 0) {
-            // Residual j (column j + 1) starts at bit j * b of the row's packed words.
-            const uint32_t k0 = seg.c0 == 0 ? 1u : 0u;
-            const uint32_t start = (seg.c0 + k0 - 1) * b;
-            uint32_t bit = start & 31u;
-            uint32_t at = row + 2 + (start >> 5);
+            // Residual j (column j + 1) starts at bit j * b of the row's packed words, so the
+            // segment's residual k (column c0 + k) starts at bit (c0 + k - 1) * b. The row's first
+            // segment thus starts b bits early, in the top of the width word: its residual 0
+            // (column 0 against itself) is zero, so every thread appends the same sequence and
+            // the width word only has zeros OR-ed into it (after this thread stored it).
+            const int32_t start = static_cast<int32_t>(seg.c0 * b) - static_cast<int32_t>(b);
+            uint32_t bit = static_cast<uint32_t>(start) & 31u;
+            uint32_t at = row + 2 + static_cast<uint32_t>(start >> 5); // row + 1 at column 0
             uint64_t acc = 0;
             // Appends `bits` bits of v (bits <= 32) and flushes a full word.
             auto append = [&](uint32_t v, uint32_t bits) {
@@ -370,22 +373,14 @@ __device__ void pack_tile(Sh &sh, uint32_t buf, uint32_t slot, const TileGeom &g
             if (!F32 && seg.n == kSeg) {
                 // uint16 (b <= 16): two residuals joined into one 2b-bit value per append.
                 const uint32_t scale = 1u << b;
-                if (k0 == 0) {
 #pragma unroll
-                    for (uint32_t k = 0; k < kSeg; k += 2) {
-                        append(z[k] + z[k + 1] * scale, 2 * b);
-                    }
-                } else {
-#pragma unroll
-                    for (uint32_t k = 1; k + 1 < kSeg; k += 2) {
-                        append(z[k] + z[k + 1] * scale, 2 * b);
-                    }
-                    append(z[kSeg - 1], b);
+                for (uint32_t k = 0; k < kSeg; k += 2) {
+                    append(z[k] + z[k + 1] * scale, 2 * b);
                 }
             } else {
 #pragma unroll
                 for (uint32_t k = 0; k < kSeg; ++k) {
-                    if (k >= k0 && k < seg.n) {
+                    if (k < seg.n) {
                         append(z[k], b);
                     }
                 }
