@@ -202,7 +202,7 @@ void ts_server_destroy(ts_server *server);
  * callers that cannot allocate device memory while they encode - a process whose GPU memory is
  * fully reserved by another allocator, an acquisition loop that must not stall on an allocator
  * or an implicit device synchronization, a deployment that forbids dynamic allocation after
- * initialization. Its scratch is a fixed 1 MiB array in device memory that the library holds
+ * initialization. Its scratch is a fixed 1056 KiB array in device memory that the library holds
  * on every GPU it is loaded on, which limits one image to ts_compress_noalloc_max_tiles()
  * tiles (131,070: for example 16384 x 32768 pixels with 128x32 tiles); larger images return
  * resource_limit and nothing is written.

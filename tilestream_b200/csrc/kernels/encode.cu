@@ -6,9 +6,9 @@
 // does all of it:
 //
 //  1. a CTA claims the next chunk of k consecutive tiles (in batch order, from an atomic
-//     counter; k = ceil(tiles / grid), at most the shared-memory payload slots: 4 uint16 or 2
-//     FP32 tiles) and, tile by tile, copies the pixels into shared memory (16-byte cp.async, the
-//     next tile in flight while the current one is encoded). Each thread takes a 16-sample
+//     counter; k = ceil(tiles / grid), at most half the shared-memory payload slots: 2 uint16
+//     or 1 FP32 tile) and, tile by tile, copies the pixels into shared memory (16-byte cp.async,
+//     the next tile in flight while the current one is encoded). Each thread takes a 16-sample
 //     segment of a row and computes its residuals in registers (zigzag mod 2^16 or XOR,
 //     encoder.cpp:32-37); the row width is the index of the highest set bit of the row's OR
 //     (docs/format.md:101), the row costs are scanned with a warp shuffle scan, and the canonical
@@ -16,16 +16,18 @@
 //     encoder.cpp:69-78). The tile is then encoded into its payload slot in shared memory: each
 //     thread appends its residuals to the row's bit stream;
 //  2. the chunk publishes the summed lengths of its tiles of its last image, in its own word and
-//     added (with an arrival count) to the word of its group of 32 chunks. One warp then sums
-//     the earlier chunks of its first image: whole groups from their group words, the chunks
-//     at either end from their own words, up to 128 words per step with every load in flight
-//     at once. Each word read is final as soon as the chunks it covers are analysed, so a
-//     look-back never waits for another look-back (a chain of inclusive prefixes advances one
-//     window per L2 round trip; a look-back per tile would wait on many more chunks).
-//     Waits are bounded and report cuda_error instead of hanging;
+//     added (with an arrival count) to the word of its group of 32 chunks. Its offsets need the
+//     lengths of the earlier chunks of its first image: whole groups from their group words, the
+//     chunks at either end from their own words. Each word read is final as soon as the chunks it
+//     covers are encoded, so a look-back never waits for another look-back (a chain of inclusive
+//     prefixes advances one window per L2 round trip; a look-back per tile would wait on many
+//     more chunks). The CTA reads them one chunk later, while it encodes its next chunk: every
+//     thread has one word in flight during that chunk's first tile. Waits are bounded and report
+//     cuda_error instead of hanging;
 //  3. the CTA writes the index entries and copies the payloads out, each word by exactly one
 //     thread (the reference's pack gathers the same bits from global memory,
-//     encoder.cu:157-173);
+//     encoder.cu:157-173), a tile of the previous chunk beside each tile of the next one, so the
+//     stores spread over the encoding instead of arriving all at once;
 //  4. the last tile of an image writes the 64-byte header and the image's DeviceResult.
 #include "ptx.cuh"
 #include "tasks.h"
@@ -45,7 +47,7 @@ constexpr uint32_t kGroupChunks = 32;
 constexpr uint64_t kGroupArrival = 1ull << 56;
 constexpr uint64_t kGroupValue = kGroupArrival - 1;
 
-constexpr uint32_t kMaxChunk = 8;
+constexpr uint32_t kMaxChunk = 2; // tiles per chunk: half the payload slots
 
 // Divides small numerators (n * d < 2^32) by d with a multiply: floor(n / d) equals the high
 // word of n * ceil(2^32 / d).
@@ -69,9 +71,25 @@ struct TileGeom {
     Divider seg_per_row; // thread segments per row
 };
 
+// A claimed chunk: tiles [first, first + count) of the batch, and what is known of them.
+struct Chunk {
+    uint64_t id;
+    uint64_t first;
+    uint32_t count;
+    uint32_t slot0;            // payload slot of its first tile
+    uint64_t carry;            // lengths of its first image's tiles in earlier chunks
+    uint64_t stop;             // the chunk holding its first image's first tile
+    uint32_t image[kMaxChunk]; // image of each tile of the chunk
+    TileGeom geom[kMaxChunk];
+    uint32_t mode_of[kMaxChunk];
+    uint32_t length_of[kMaxChunk];
+    uint64_t offset[kMaxChunk]; // payload offset within its image's payload area, less the carry
+};
+
 // Words: the largest tile in 32-bit words, 2048 for uint16-only batches (4096 samples) and
 // 4096 when the batch has FP32 images; a PREDICT payload is always shorter than the RAW one.
-// Slots: payloads of a chunk kept until its offsets are known (the most tiles in a chunk).
+// Slots: payloads kept until their offsets are known, for two chunks (the one being encoded
+// and the one before it, written out meanwhile).
 template <uint32_t Words, uint32_t Slots> struct EncodeShared {
     static constexpr uint32_t kSlots = Slots;
     // Two tile buffers: the tile being analysed and the next one in flight. Rows are packed
@@ -83,15 +101,8 @@ template <uint32_t Words, uint32_t Slots> struct EncodeShared {
     uint32_t row_word[TSK_MAX_ROWS + 1]; // first payload word of each row
     uint32_t mode;
     uint32_t length;
-    // The claimed chunk: tiles [first, first + count) of the batch.
-    uint64_t chunk;
-    uint64_t first;
-    uint32_t count;
-    uint32_t image[kMaxChunk];  // image of each tile of the chunk
-    TileGeom geom[kMaxChunk];
-    uint32_t mode_of[kMaxChunk];
-    uint32_t length_of[kMaxChunk];
-    uint64_t offset[kMaxChunk]; // payload offset of each tile within its image's payload area
+    // The chunk being encoded, the one before it and the next one, in rotation.
+    Chunk chunks[3];
 };
 
 // Residual of a sample against its left neighbour: for uint16 the zigzag of the difference
@@ -106,14 +117,16 @@ template <bool F32> __device__ __forceinline__ uint32_t residual(uint32_t cur, u
     }
 }
 
-__device__ __forceinline__ uint64_t ld_acquire(const uint64_t *p) {
+// Look-back words carry their own values (nothing else is read on the strength of one), so
+// relaxed device-scope accesses suffice; a relaxed load does not hold back the loads after it.
+__device__ __forceinline__ uint64_t ld_relaxed(const uint64_t *p) {
     uint64_t v;
-    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
     return v;
 }
 
-__device__ __forceinline__ void st_release(uint64_t *p, uint64_t v) {
-    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+__device__ __forceinline__ void st_relaxed(uint64_t *p, uint64_t v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
 __device__ __forceinline__ void put_word(uint8_t *file, uint64_t byte, uint32_t v) {
@@ -492,54 +505,69 @@ struct SingleImage {
     }
 };
 
-// Sums the lengths published by chunks [stop, g), warp 0 only. Whole groups inside the range
-// are read from their group words, the chunks before the first whole group and after the last
-// one from their own words: the words are numbered 0 .. n-1 in that order and each lane loads
-// up to kPerLane of every 32 * kPerLane before it waits on any.
+// The words whose sum is the lengths published by chunks [stop, g): whole groups inside the
+// range from their group words, the chunks before the first whole group and after the last one
+// from their own words, numbered 0 .. n-1 in that order (none when stop == g).
+struct LookBack {
+    const uint64_t *flags, *groups;
+    uint64_t stop, lo, head, mid, tail_first, n;
+    __device__ LookBack(const uint64_t *f, const uint64_t *gr, uint64_t g, uint64_t s)
+        : flags(f), groups(gr), stop(s) {
+        lo = (s + kGroupChunks - 1) / kGroupChunks;
+        const uint64_t hi = g / kGroupChunks;
+        const bool whole = lo < hi;
+        head = whole ? lo * kGroupChunks - s : g - s; // chunks from stop
+        mid = whole ? hi - lo : 0;                    // groups from lo
+        tail_first = whole ? hi * kGroupChunks : g;   // chunks to g
+        n = head + mid + (g - tail_first);
+    }
+    __device__ const uint64_t *word(uint64_t i) const {
+        return i < head        ? flags + stop + i
+               : i < head + mid ? groups + lo + (i - head)
+                                : flags + tail_first + (i - head - mid);
+    }
+    // The value of word i, given a first load v: reloaded until complete, for a bounded time
+    // (then `late` is set and 0 returned).
+    __device__ uint64_t value(uint64_t i, uint64_t v, bool &late) const {
+        const bool group = i >= head && i < head + mid;
+        auto ready = [&](uint64_t w) {
+            return group ? (w >> 56) == kGroupChunks : (w >> 62) != 0;
+        };
+        uint32_t spins = 0;
+        while (!ready(v) && spins < (1u << 22)) {
+            __nanosleep(64);
+            v = ld_relaxed(word(i));
+            ++spins;
+        }
+        if (!ready(v)) {
+            late = true;
+            return 0;
+        }
+        return group ? (v & kGroupValue) : (v & kValue);
+    }
+};
+
+// Sums the lengths published by chunks [stop, g), warp 0 only: each lane loads up to kPerLane of
+// every 32 * kPerLane words before it waits on any.
 __device__ uint64_t look_back(const uint64_t *flags, const uint64_t *groups, uint64_t g,
                               uint64_t stop, bool &timed_out) {
     constexpr uint32_t kPerLane = 4;
     const uint32_t lane = threadIdx.x % 32;
-    const uint64_t lo = (stop + kGroupChunks - 1) / kGroupChunks, hi = g / kGroupChunks;
-    const bool whole = lo < hi;
-    const uint64_t head = whole ? lo * kGroupChunks - stop : g - stop; // chunks from stop
-    const uint64_t mid = whole ? hi - lo : 0;                          // groups from lo
-    const uint64_t tail_first = whole ? hi * kGroupChunks : g;          // chunks to g
-    const uint64_t n = head + mid + (g - tail_first);
-    auto word = [&](uint64_t i) -> const uint64_t * {
-        return i < head        ? flags + stop + i
-               : i < head + mid ? groups + lo + (i - head)
-                                : flags + tail_first + (i - head - mid);
-    };
+    const LookBack lb(flags, groups, g, stop);
     uint64_t sum = 0;
     bool late = false;
-    for (uint64_t base = 0; base < n; base += 32 * kPerLane) {
+    for (uint64_t base = 0; base < lb.n; base += 32 * kPerLane) {
         uint64_t v[kPerLane];
 #pragma unroll
         for (uint32_t k = 0; k < kPerLane; ++k) {
             const uint64_t i = base + k * 32 + lane;
-            v[k] = i < n ? ld_acquire(word(i)) : 0;
+            v[k] = i < lb.n ? ld_relaxed(lb.word(i)) : 0;
         }
 #pragma unroll
         for (uint32_t k = 0; k < kPerLane; ++k) {
             const uint64_t i = base + k * 32 + lane;
-            if (i >= n) {
-                continue;
-            }
-            const bool group = i >= head && i < head + mid;
-            auto ready = [&](uint64_t w) {
-                return group ? (w >> 56) == kGroupChunks : (w >> 62) != 0;
-            };
-            uint32_t spins = 0;
-            while (!ready(v[k]) && spins < (1u << 22)) {
-                __nanosleep(64);
-                v[k] = ld_acquire(word(i));
-                ++spins;
-            }
-            if (!ready(v[k])) {
-                late = true;
-            } else {
-                sum += group ? (v[k] & kGroupValue) : (v[k] & kValue);
+            if (i < lb.n) {
+                sum += lb.value(i, v[k], late);
             }
         }
     }
@@ -547,157 +575,237 @@ __device__ uint64_t look_back(const uint64_t *flags, const uint64_t *groups, uin
     return warp_sum64(sum);
 }
 
-// The persistent loop: claim a chunk, analyse its tiles, publish, look back, write.
+// The persistent loop. A CTA encodes its chunk c tile by tile; meanwhile it finishes its
+// previous chunk c': while c's first tile is analysed, every thread has one word of c''s
+// look-back in flight (c' was published a whole chunk earlier, so the chunks before it have
+// published theirs), and each later tile of c comes with one tile of c' written out. Then c is
+// published and the next chunk, claimed at c's last tile, starts copying in.
 template <bool AnyF32, typename Sh, typename Images>
 __device__ void encode_chunks(Sh &sh, const Images &images, uint64_t total_tiles,
                               uint32_t chunk_tiles, uint64_t *state, tsk_result *results) {
     uint64_t *counter = state;
     uint64_t *flags = state + 2;
     uint64_t *groups = flags + (total_tiles + chunk_tiles - 1) / chunk_tiles;
-    const uint32_t warp = threadIdx.x / 32;
-    for (;;) {
-        if (threadIdx.x == 0) {
-            const uint64_t g = atomicAdd(reinterpret_cast<unsigned long long *>(counter), 1ull);
-            const uint64_t first = g * chunk_tiles;
-            sh.chunk = g;
-            sh.first = first;
-            sh.count = first < total_tiles
-                           ? static_cast<uint32_t>(total_tiles - first < chunk_tiles
-                                                       ? total_tiles - first
-                                                       : chunk_tiles)
-                           : 0u;
+    const uint32_t warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    constexpr uint32_t kNone = 3;
+
+    // Thread 0 claims the next chunk into record m.
+    auto claim = [&](uint32_t m) {
+        const uint64_t g = atomicAdd(reinterpret_cast<unsigned long long *>(counter), 1ull);
+        const uint64_t first = g * chunk_tiles;
+        Chunk &c = sh.chunks[m];
+        c.id = g;
+        c.first = first;
+        c.count = first < total_tiles ? static_cast<uint32_t>(total_tiles - first < chunk_tiles
+                                                                  ? total_tiles - first
+                                                                  : chunk_tiles)
+                                      : 0u;
+    };
+    // Thread `t` (t < count) places tile t of claimed chunk m.
+    auto place = [&](uint32_t m, uint32_t t) {
+        Chunk &c = sh.chunks[m];
+        const uint32_t im = images.owner(c.first + t);
+        c.image[t] = im;
+        c.geom[t] = tile_geom(images[im], c.first + t - images[im].first_tile);
+    };
+    // Copies tile t of chunk m into buffer `buf` (a cp.async group is closed either way).
+    auto prefetch = [&](uint32_t m, uint32_t t, uint32_t buf) {
+        const Chunk &c = sh.chunks[m];
+        if (t < c.count) {
+            issue_tile_any<AnyF32>(sh, buf, images[c.image[t]], c.geom[t]);
+        } else {
+            cp_async_commit();
         }
-        __syncthreads();
-        const uint32_t count = sh.count;
-        if (count == 0) {
+    };
+    // Warp 0: chunk m's offsets within its images, and the lengths of its last image's tiles
+    // published in its own word and added to its group's.
+    auto publish = [&](uint32_t m) {
+        Chunk &c = sh.chunks[m];
+        if (lane == 0) {
+            uint64_t run = 0;
+            for (uint32_t i = 0; i < c.count; ++i) {
+                if (i != 0 && c.image[i] != c.image[i - 1]) {
+                    run = 0;
+                }
+                c.offset[i] = run;
+                run += c.length_of[i];
+            }
+            c.carry = 0;
+            c.stop = images[c.image[0]].first_tile / chunk_tiles;
+            st_relaxed(flags + c.id, kPublished | run);
+            atomicAdd(reinterpret_cast<unsigned long long *>(groups + c.id / kGroupChunks),
+                      static_cast<unsigned long long>(kGroupArrival | run));
+        }
+    };
+    // The look-back of chunk m: the chunks of its first image before it (none when the image
+    // begins in m).
+    auto look_back_of = [&](uint32_t m) {
+        const Chunk &c = sh.chunks[m];
+        return LookBack(flags, groups, c.id, c.stop);
+    };
+    // Every thread: word threadIdx.x of chunk m's look-back, loaded early.
+    auto early_load = [&](uint32_t m) -> uint64_t {
+        const LookBack lb = look_back_of(m);
+        return threadIdx.x < lb.n ? ld_relaxed(lb.word(threadIdx.x)) : 0ull;
+    };
+    // Every thread: its words of chunk m's look-back (the first one given), summed into the
+    // chunk's carry; a wait that runs out marks the image's result cuda_error.
+    auto settle = [&](uint32_t m, uint64_t early) {
+        const LookBack lb = look_back_of(m);
+        if (lb.n == 0) {
             return;
         }
-        const uint64_t g = sh.chunk, first = sh.first;
-        if (threadIdx.x < count) {
-            const uint32_t m = images.owner(first + threadIdx.x);
-            sh.image[threadIdx.x] = m;
-            sh.geom[threadIdx.x] = tile_geom(images[m], first + threadIdx.x - images[m].first_tile);
+        bool late = false;
+        uint64_t sum = 0;
+        for (uint64_t i = threadIdx.x; i < lb.n; i += kThreads) {
+            sum += lb.value(i, i == threadIdx.x ? early : ld_relaxed(lb.word(i)), late);
         }
-        if (threadIdx.x < TSK_MAX_ROWS) {
-            sh.row_or[threadIdx.x] = 0;
-        }
-        __syncthreads();
-
-        // Tile i of the chunk: its image and its geometry.
-        auto tile = [&](uint32_t i, const tsk_encode_image *&im,
-                        uint64_t &index) -> const TileGeom & {
-            im = &images[sh.image[i]];
-            index = sh.geom[i].index;
-            return sh.geom[i];
-        };
-        // Copies tile i into buffer i % 2 (a cp.async group is closed either way).
-        auto prefetch = [&](uint32_t i) {
-            if (i < count) {
-                const tsk_encode_image *im;
-                uint64_t index;
-                const TileGeom &geom = tile(i, im, index);
-                issue_tile_any<AnyF32>(sh, i % 2, *im, geom);
-            } else {
-                cp_async_commit();
+        sum = warp_sum64(sum);
+        late = __any_sync(0xffffffffu, late);
+        if (lane == 0) {
+            if (sum != 0) {
+                atomicAdd(reinterpret_cast<unsigned long long *>(&sh.chunks[m].carry),
+                          static_cast<unsigned long long>(sum));
             }
-        };
+            if (late) {
+                atomicCAS(&results[sh.chunks[m].image[0]].status, 0u, 9u);
+            }
+        }
+    };
+    // Tile i of chunk m (its carry complete): index entry and payload; the last tile of an
+    // image writes its header.
+    auto write_out = [&](uint32_t m, uint32_t i) {
+        const Chunk &c = sh.chunks[m];
+        const uint32_t im = c.image[i];
+        const tsk_encode_image &image = images[im];
+        const TileGeom &geom = c.geom[i];
+        const uint64_t at = c.offset[i] + (im == c.image[0] ? c.carry : 0);
+        store_tile(sh, c.slot0 + i, image, geom.index, geom, c.mode_of[i], c.length_of[i],
+                   64 + 32 * image.tile_count + at);
+        if (geom.index + 1 == image.tile_count) {
+            write_header(image, at + c.length_of[i], results + im);
+        }
+    };
 
-        // 1. Encode the chunk's tiles into their payload slots; tile i + 1 is copied while tile i
-        //    is encoded.
-        prefetch(0);
+    uint32_t cur = 0, prev = kNone, next = 1; // chunk records
+    if (threadIdx.x == 0) {
+        claim(cur);
+        sh.chunks[cur].slot0 = 0;
+    }
+    if (threadIdx.x < TSK_MAX_ROWS) {
+        sh.row_or[threadIdx.x] = 0; // then cleared after each tile
+    }
+    __syncthreads();
+    if (sh.chunks[cur].count == 0) {
+        return;
+    }
+    if (threadIdx.x < sh.chunks[cur].count) {
+        place(cur, threadIdx.x);
+    }
+    __syncthreads();
+    uint32_t buf = 0; // tile buffer of the next tile to encode
+    prefetch(cur, 0, buf);
+    for (;;) {
+        Chunk &c = sh.chunks[cur];
+        const uint32_t count = c.count;
+        const uint32_t before = prev != kNone ? sh.chunks[prev].count : 0u; // tiles of c'
+        uint64_t early = 0;
         for (uint32_t i = 0; i < count; ++i) {
+            const uint32_t slot = c.slot0 + i;
             for (uint32_t k = threadIdx.x; k < sizeof(sh.payload[0]) / 16; k += kThreads) {
-                reinterpret_cast<uint4 *>(sh.payload[i])[k] = make_uint4(0, 0, 0, 0);
+                reinterpret_cast<uint4 *>(sh.payload[slot])[k] = make_uint4(0, 0, 0, 0);
             }
             cp_async_wait<0>();
-            // Tile i has landed, and every thread is done with tile i - 1 (its buffer is free).
+            // Tile i has landed, and every thread is done with the tile before it (its buffer
+            // is free).
             __syncthreads();
-            prefetch(i + 1);
-            const tsk_encode_image *im;
-            uint64_t index;
-            const TileGeom &geom = tile(i, im, index);
+            if (i + 1 < count) {
+                prefetch(cur, i + 1, buf ^ 1);
+            } else if (threadIdx.x == 0) {
+                claim(next);
+            }
+            if (i == 0 && before != 0) {
+                early = early_load(prev);
+            }
+            if (i >= 1 && i - 1 < before) {
+                write_out(prev, i - 1); // its carry was settled at tile 0
+            }
+            const tsk_encode_image &im = images[c.image[i]];
+            const TileGeom &geom = c.geom[i];
             const Segment seg = segment_of(geom);
             uint32_t z[kSeg];
-            if (AnyF32 && im->type == 2) {
-                analyze_tile<AnyF32>(sh, i % 2, geom, seg, z);
-                pack_tile<AnyF32>(sh, i % 2, i, geom, seg, z);
+            if (AnyF32 && im.type == 2) {
+                analyze_tile<AnyF32>(sh, buf, geom, seg, z);
+                pack_tile<AnyF32>(sh, buf, slot, geom, seg, z);
             } else {
-                analyze_tile<false>(sh, i % 2, geom, seg, z);
-                pack_tile<false>(sh, i % 2, i, geom, seg, z);
+                analyze_tile<false>(sh, buf, geom, seg, z);
+                pack_tile<false>(sh, buf, slot, geom, seg, z);
             }
             if (threadIdx.x == 0) {
-                sh.mode_of[i] = sh.mode;
-                sh.length_of[i] = sh.length;
+                c.mode_of[i] = sh.mode;
+                c.length_of[i] = sh.length;
             }
             if (threadIdx.x < TSK_MAX_ROWS) {
                 sh.row_or[threadIdx.x] = 0; // for the next tile (read before the last barrier)
             }
+            if (i == 0 && before != 0) {
+                settle(prev, early);
+            }
+            buf ^= 1;
         }
-        cp_async_wait<0>();
         __syncthreads();
-
-        // 2. Offsets: within the chunk, then the carry of the first image from earlier chunks.
+        // The rest of c' (its carry is complete); then c is published while the next chunk's
+        // tiles are placed, and its first tile starts copying in.
+        for (uint32_t j = count - 1; j < before; ++j) {
+            write_out(prev, j);
+        }
+        const uint32_t next_count = sh.chunks[next].count;
         if (warp == 0) {
-            const uint32_t lane = threadIdx.x % 32;
-            const uint32_t first_image = sh.image[0];
-            uint64_t tail = 0; // lengths of the last image's tiles in this chunk
-            if (lane == 0) {
-                uint64_t run = 0;
-                for (uint32_t i = 0; i < count; ++i) {
-                    if (i != 0 && sh.image[i] != sh.image[i - 1]) {
-                        run = 0;
-                    }
-                    sh.offset[i] = run;
-                    run += sh.length_of[i];
-                }
-                tail = run;
-            }
-            __syncwarp();
-            tail = __shfl_sync(0xffffffffu, tail, 0);
-            const uint64_t image_first = images[first_image].first_tile;
-            if (lane == 0) {
-                st_release(flags + g, kPublished | tail);
-                atomicAdd(reinterpret_cast<unsigned long long *>(groups + g / kGroupChunks),
-                          static_cast<unsigned long long>(kGroupArrival | tail));
-            }
-            uint64_t carry = 0;
-            if (image_first < first) { // the first image began in an earlier chunk
-                bool timed_out = false;
-                carry = look_back(flags, groups, g, image_first / chunk_tiles, timed_out);
-                if (lane == 0 && timed_out) {
-                    atomicCAS(&results[first_image].status, 0u, 9u);
-                }
-            }
-            __syncwarp();
-            if (lane < count && sh.image[lane] == first_image) {
-                sh.offset[lane] += carry;
-            }
+            publish(cur);
+        } else if (threadIdx.x - 32 < next_count) {
+            place(next, threadIdx.x - 32);
         }
         __syncthreads();
-
-        // 3. Index entries and payloads; the last tile of an image writes its header.
-        for (uint32_t i = 0; i < count; ++i) {
-            const uint32_t m = sh.image[i];
-            const tsk_encode_image *im;
-            uint64_t index;
-            const TileGeom &geom = tile(i, im, index);
-            const uint64_t offset = 64 + 32 * im->tile_count + sh.offset[i];
-            store_tile(sh, i, *im, index, geom, sh.mode_of[i], sh.length_of[i], offset);
-            if (index + 1 == im->tile_count) {
-                write_header(*im, sh.offset[i] + sh.length_of[i], results + m);
-            }
+        prefetch(next, 0, buf);
+        if (threadIdx.x == 0) {
+            sh.chunks[next].slot0 = c.slot0 == 0 ? Sh::kSlots / 2 : 0; // the slots of c'
+        }
+        const uint32_t spare = prev != kNone ? prev : 2;
+        prev = cur;
+        cur = next;
+        next = spare;
+        if (next_count == 0) {
+            break;
         }
         __syncthreads();
     }
+    // The last chunk: its look-back by warp 0, then its tiles.
+    if (warp == 0) {
+        const Chunk &c = sh.chunks[prev];
+        bool timed_out = false;
+        const uint64_t carry = look_back(flags, groups, c.id, c.stop, timed_out);
+        if (lane == 0) {
+            sh.chunks[prev].carry = carry;
+            if (timed_out) {
+                atomicCAS(&results[c.image[0]].status, 0u, 9u);
+            }
+        }
+    }
+    __syncthreads();
+    for (uint32_t j = 0; j < sh.chunks[prev].count; ++j) {
+        write_out(prev, j);
+    }
 }
 
-// AnyF32: the batch has FP32 images (16 KiB tile buffers and payload slots, two tiles per
-// chunk: 64 KiB); otherwise 8 KiB buffers and slots, four tiles per chunk (48 KiB), four CTAs
-// per SM.
+// AnyF32: the batch has FP32 images (16 KiB tile buffers and payload slots, two slots: one-tile
+// chunks, 64 KiB, three CTAs per SM); otherwise 8 KiB buffers and slots, four slots: two-tile
+// chunks (48 KiB), four CTAs per SM.
 template <bool AnyF32> using SharedFor = EncodeShared<AnyF32 ? 4096u : 2048u, AnyF32 ? 2u : 4u>;
+static_assert(SharedFor<false>::kSlots / 2 <= kMaxChunk && SharedFor<true>::kSlots / 2 >= 1,
+              "a chunk's tiles fit half the payload slots");
 
 template <bool AnyF32>
-__global__ void __launch_bounds__(kThreads, AnyF32 ? 1 : 4)
+__global__ void __launch_bounds__(kThreads, AnyF32 ? 3 : 4)
     encode_kernel(const tsk_encode_image *__restrict__ images, uint32_t image_count,
                   uint64_t total_tiles, uint32_t chunk_tiles, uint64_t *state,
                   tsk_result *results) {
@@ -708,9 +816,9 @@ __global__ void __launch_bounds__(kThreads, AnyF32 ? 1 : 4)
 }
 
 // Tiles per chunk for a launch of `grid` CTAs: as many as spread the tiles over the grid in one
-// round, at most the instance's payload slots (larger batches take several rounds).
+// round, at most half the instance's payload slots (larger batches take several rounds).
 uint32_t chunk_tiles_for(uint64_t total_tiles, uint64_t grid, bool any_f32) {
-    const uint64_t most = any_f32 ? SharedFor<true>::kSlots : SharedFor<false>::kSlots;
+    const uint64_t most = (any_f32 ? SharedFor<true>::kSlots : SharedFor<false>::kSlots) / 2;
     const uint64_t k = (total_tiles + grid - 1) / grid;
     return static_cast<uint32_t>(k < 1 ? 1 : (k > most ? most : k));
 }
@@ -783,15 +891,16 @@ extern "C" int tsk_encode_launch(const tsk_encode_image *images, uint32_t image_
 namespace tsk {
 namespace {
 
-// 1 MiB of state: two words, one per chunk and one per 32 chunks. An image with more tiles than
-// the grid has CTAs takes two tiles per chunk at least, so the largest accepted one (131,070
-// tiles) needs at most 67,585 words; an image with fewer tiles than CTAs has a chunk per tile.
-constexpr uint64_t kStaticStateWords = 131072;
+// At most kStaticMaxTiles tiles per image. The state is two words, one per chunk and one per 32
+// chunks; a chunk holds one tile at least, so 131,070 tiles need at most 2 + 131,070 + 4,096
+// words: 1056 KiB.
+constexpr uint64_t kStaticMaxTiles = 131070;
+constexpr uint64_t kStaticStateWords = 2 + kStaticMaxTiles + (kStaticMaxTiles + 31) / 32;
 
 __device__ __align__(256) uint64_t g_encode_scratch[kStaticStateWords];
 
 template <bool AnyF32>
-__global__ void __launch_bounds__(kThreads, AnyF32 ? 1 : 4)
+__global__ void __launch_bounds__(kThreads, AnyF32 ? 3 : 4)
     encode_kernel_static(const __grid_constant__ tsk_encode_image image, uint64_t total_tiles,
                          uint32_t chunk_tiles, uint64_t *state, tsk_result *result) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
@@ -842,7 +951,7 @@ cudaError_t static_setup(int device, StaticSetup &out) {
 } // namespace tsk
 
 extern "C" uint64_t tsk_encode_static_max_tiles(void) {
-    return tsk::kStaticStateWords - 2;
+    return tsk::kStaticMaxTiles;
 }
 
 // Encodes one validated image with the static scratch; allocates nothing. Returns a
