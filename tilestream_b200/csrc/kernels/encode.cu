@@ -811,8 +811,25 @@ __global__ void __launch_bounds__(kThreads, AnyF32 ? 3 : 4)
                   tsk_result *results) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
     auto &sh = *reinterpret_cast<SharedFor<AnyF32> *>(smem_raw);
+    griddep_wait(); // the state and the result records are cleared by encode_clear_kernel
     encode_chunks<AnyF32>(sh, ImageTable{images, image_count}, total_tiles, chunk_tiles, state,
                           results);
+}
+
+// Clears a launch's look-back state and its images' result records in one small launch (two
+// memsets would be two graph nodes with their own gaps), and lets the encode kernel that
+// follows start launching at once: it waits for this grid before it reads either.
+__global__ void encode_clear_kernel(uint64_t *state, uint64_t words, tsk_result *results,
+                                    uint32_t count) {
+    griddep_launch_dependents();
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    const uint64_t first = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    for (uint64_t i = first; i < words; i += stride) {
+        state[i] = 0;
+    }
+    for (uint64_t i = first; i < count; i += stride) {
+        results[i] = tsk_result{0, 0, 0};
+    }
 }
 
 // Tiles per chunk for a launch of `grid` CTAs: as many as spread the tiles over the grid in one
@@ -851,10 +868,8 @@ extern "C" int tsk_encode_launch(const tsk_encode_image *images, uint32_t image_
                                  uint64_t total_tiles, uint32_t any_float, void *state,
                                  tsk_result *results, cudaStream_t stream) {
     if (total_tiles == 0) return cudaSuccess;
-    cudaError_t e = cudaMemsetAsync(results, 0, sizeof(tsk_result) * image_count, stream);
-    if (e != cudaSuccess) return e;
     int device = 0, sms = 0, per_sm = 0;
-    e = cudaGetDevice(&device);
+    cudaError_t e = cudaGetDevice(&device);
     if (e != cudaSuccess) return e;
     e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     if (e != cudaSuccess) return e;
@@ -866,11 +881,25 @@ extern "C" int tsk_encode_launch(const tsk_encode_image *images, uint32_t image_
     const uint32_t k = tsk::chunk_tiles_for(total_tiles, grid, any_float != 0);
     const uint64_t chunks = (total_tiles + k - 1) / k;
     if (grid > chunks) grid = chunks;
-    e = cudaMemsetAsync(state, 0, 8 * tsk::state_words(chunks), stream);
+    uint64_t *words = static_cast<uint64_t *>(state);
+    const uint64_t nwords = tsk::state_words(chunks);
+    const uint64_t clear = nwords > image_count ? nwords : image_count;
+    const uint32_t clear_grid = static_cast<uint32_t>(clear / 256 + 1 < 1024 ? clear / 256 + 1 : 1024);
+    tsk::encode_clear_kernel<<<clear_grid, 256, 0, stream>>>(words, nwords, results, image_count);
+    e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    kernel<<<static_cast<uint32_t>(grid), tsk::kThreads, smem, stream>>>(
-        images, image_count, total_tiles, k, static_cast<uint64_t *>(state), results);
-    return cudaGetLastError();
+    // Programmatic dependent launch: the encode grid is scheduled while the clear runs.
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(static_cast<uint32_t>(grid));
+    cfg.blockDim = dim3(tsk::kThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, images, image_count, total_tiles, k, words, results);
 }
 
 // ---------------------------------------------------------------------------------------------
