@@ -95,7 +95,7 @@ template <uint32_t Words, uint32_t Slots> struct EncodeShared {
     // Two tile buffers: the tile being analysed and the next one in flight. Rows are packed
     // (w samples each), as uint16 or FP32 words.
     alignas(16) uint32_t raw[2][Words];
-    alignas(16) uint32_t payload[Slots][Words]; // the chunk's encoded payloads
+    alignas(16) uint32_t payload[Slots][Words]; // encoded payloads of the two chunks
     uint32_t row_or[TSK_MAX_ROWS];         // OR of each row's residuals
     uint32_t bits[TSK_MAX_ROWS];
     uint32_t row_word[TSK_MAX_ROWS + 1]; // first payload word of each row
