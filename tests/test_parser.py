@@ -47,6 +47,26 @@ def test_valid_files_tables_match(oracle_lib):
         assert check(oracle_lib, file, None) == 0
 
 
+def test_large_files_tables_match_reference(oracle_lib, reference):
+    """4096x4096 frames (4096 tiles each): the payloads are checked in ranges of tiles on
+    several host threads; the tables must equal the reference parser's, and a bad row in the
+    last tile must still be found."""
+    frame = workloads.detector_frame(4096, 4096, seed=2)
+    for tile in api.TILE_SHAPES:
+        file = oracle_lib.compress_image(frame, tile)
+        st, meta = ours(file)
+        want, ref_meta = reference.parse(file)
+        assert st == want == 0
+        same_tables(meta, ref_meta)
+        tiles, segments = meta.tiles, meta.segments
+        last = len(tiles) - 1
+        assert int(tiles["mode"][last]) == 2
+        seg = segments[int(tiles["first_segment"][last]) + int(tiles["height"][last]) - 1]
+        bad = bytearray(file)
+        bad[int(tiles["offset"][last]) + int(seg["payload_offset"]) - 8 + 6] = 0x40
+        assert ours(bytes(bad))[0] == reference.parse(bytes(bad))[0] == int(Status.malformed_data)
+
+
 def test_every_truncation(oracle_lib):
     frame = workloads.detector_frame(300, 70, seed=4)
     file = oracle_lib.compress_image(frame, (64, 64))
@@ -96,6 +116,32 @@ def test_limits(oracle_lib):
         assert st == want == int(Status.resource_limit)
     st, _ = ours(file, ParseLimits(len(file), 21, big))  # 3 x 7 tiles of 128x32
     assert st == 0
+
+
+def test_malformed_payload_outranks_segment_budget(oracle_lib, reference):
+    """A file over the row-segment budget whose payload is also malformed reports
+    malformed_data: every payload is checked before that budget (reference
+    src/cpu/parser.cpp:86-171 walks the payloads before it sizes the segment table)."""
+    frame = workloads.detector_frame(300, 200, seed=6)
+    file = oracle_lib.compress_image(frame)
+    st, meta = ours(file)
+    assert st == 0
+    tiles, segments = meta.tiles, meta.segments
+    predict = [i for i in range(len(tiles)) if int(tiles["mode"][i]) == 2]
+    last = predict[-1]
+    # A segment's payload_offset is that of its packed words, just after its 8-byte descriptor.
+    seg = segments[int(tiles["first_segment"][last])]
+    desc = int(tiles["offset"][last]) + int(seg["payload_offset"]) - 8
+    bad = bytearray(file)
+    bad[desc + 5] = 1  # a reserved byte of the last PREDICT tile's first row descriptor
+    big = 2 ** 63 - 1
+    # Room for the 21 tile records (72 + 32 * 21 bytes) but not for the file's row segments.
+    tight = (big, big, 72 + 32 * 21 + 24 * 10)
+    for candidate, want in ((file, Status.resource_limit), (bytes(bad), Status.malformed_data)):
+        got, _ = ours(candidate, ParseLimits(*tight))
+        assert got == int(want)
+        assert oracle_lib.parse(candidate, tight)[0] == int(want)
+        assert reference.parse(candidate, tight)[0] == int(want)
 
 
 def test_empty_and_null_sources():
