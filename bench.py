@@ -401,16 +401,44 @@ def run_e2e(args, torch, stream, shapes, wsb, recs):
             "ms_per_step": round(ms / steps, 4), "streams": len(streams)}
 
 
+def best_ms(fn, reps: int = 10) -> float:
+    best = float("inf")
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        fn()
+        best = min(best, time.perf_counter() - t0)
+    return best * 1e3
+
+
+def host_parse(shapes):
+    """parse_metadata of the three archives through the product API (best of 10 each)."""
+    from tilestream_b200 import api
+    out = {}
+    for s in shapes:
+        src = np.frombuffer(s["file"], dtype=np.uint8)
+        out["%dx%d" % s["tile"]] = round(best_ms(lambda: api.parse_metadata(src)), 3)
+    return {"unit": "ms per 4096x4096 archive (20 MB, 4096 tiles)", "ms": out,
+            "threads": min(8, os.cpu_count() or 1)}
+
+
 def cpu_baseline(shapes, seconds):
     import oracle
     archive = shapes[0]["file"]
     ref = oracle.Reference.available()
     threads = os.cpu_count() or 1
     rate, images = cpu_decode_rate(archive, seconds, threads, ref)
-    return {"value": round(rate / 1e9, 3), "unit": "GB/s", "cores": threads,
+    line = {"value": round(rate / 1e9, 3), "unit": "GB/s", "cores": threads,
             "kind": "reference" if ref else "port",
             "sample": f"{images} decodes of the 4096x4096 uint16 128x32 archive, one image per "
                       f"thread, {seconds:.0f} s"}
+    one, images1 = cpu_decode_rate(archive, max(1.0, seconds / 5), 1, ref)
+    line["single_thread"] = {"value": round(one / 1e9, 3), "unit": "GB/s",
+                             "sample": f"{images1} decodes on one thread"}
+    if ref:
+        codec = oracle.Reference()
+        line["parse_ms"] = {"%dx%d" % s["tile"]: round(best_ms(
+            lambda s=s: codec.parse_status(s["file"])), 3) for s in shapes}
+    return line
 
 
 def run_reference(args):
@@ -1007,6 +1035,7 @@ def main():
             line["batched_decode"] = run_batched(args, torch, stream, peak)
         if "serving" in sections:
             line["serving"] = run_serving(args, torch, stream)
+        line["host_parse"] = host_parse(shapes)
         line["cpu_baseline"] = cpu_baseline(shapes, args.cpu_seconds)
         print(json.dumps(line), flush=True)
     if world > 1:

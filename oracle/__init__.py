@@ -279,6 +279,12 @@ class Reference:
                                      pitch, out.size, _ptr(lim))
         return st, out
 
+    def parse_status(self, file: bytes) -> int:
+        """One reference parse_metadata call (its tables are built, not copied out)."""
+        src = np.frombuffer(file, dtype=np.uint8) if len(file) else np.zeros(1, np.uint8)
+        info = np.zeros(8, dtype=np.uint64)
+        return self.lib.tsr_parse(_ptr(src), len(file), None, _ptr(info), None, 0, None, 0)
+
     def parse(self, file: bytes, limits=None):
         src = np.frombuffer(file, dtype=np.uint8) if len(file) else np.zeros(1, np.uint8)
         lim = np.array(limits, dtype=np.uint64) if limits is not None else None
