@@ -652,6 +652,171 @@ def run_calibrated(args, torch, stream, peak):
                 "equals_fused_bit_for_bit": standalone_same}}
 
 
+def run_archive_roi(args, torch, shapes):
+    """ROIs of archives held in pinned host memory, decoded with calibration into FP32 on the
+    device (the reference benchmark's archive ROI mode, benchmarks/codec_benchmark.cpp:153-320).
+    Per request: the ROI's tile payloads are copied to the device on a copy stream, a plan is
+    prepared on its own stream, and decode_calibrate runs on a compute stream after the copy's
+    event; requests pipeline (the host enqueues request k + 1 while the device works on k).
+    Three ways to get the payloads to the device are timed: `direct` (stage_roi_tiles: one copy
+    per tile row straight from the pinned archive), `gather` (the reference's way: host copies
+    of the ROI's tiles into a pinned staging buffer, then one copy) and `whole_archive` (the
+    whole file copied per request). Decoded bytes count ROI pixels at 2 B (the stored type)."""
+    from tilestream_b200 import api, cuda
+    from tilestream_b200.api import (BatchItem, Calibration, CompressedInput, ConstBytes,
+                                     MutableBytes, Roi, Status, TileMapping)
+    rng = np.random.default_rng(17)
+    n = 64
+    pinned = [torch.from_numpy(np.frombuffer(s["file"], dtype=np.uint8).copy()).pin_memory()
+              for s in shapes]
+    reqs = []
+    for k in range(n):
+        a = k % len(shapes)
+        w = int(np.exp(rng.uniform(np.log(128), np.log(2048))))
+        h = int(np.exp(rng.uniform(np.log(128), np.log(2048))))
+        x, y = int(rng.integers(0, W - w + 1)), int(rng.integers(0, H - h + 1))
+        reqs.append((a, (x, y, w, h)))
+    copy, prep, compute = torch.cuda.Stream(), torch.cuda.Stream(), torch.cuda.Stream()
+    slots = []
+    for a, roi in reqs:
+        meta = shapes[a]["meta"]
+        st, need = cuda.roi_staging_size(meta, Roi(*roi))
+        assert st == Status.success
+        slots.append({
+            "need": need, "staging": torch.empty(need.bytes, dtype=torch.uint8, device="cuda"),
+            "host_staging": torch.empty(need.bytes, dtype=torch.uint8).pin_memory(),
+            "maps": (TileMapping * need.tiles)(),
+            "out": torch.empty(roi[2] * roi[3] * 4, dtype=torch.uint8, device="cuda"),
+            # the whole-archive way: a device copy of the archive per request
+            "archive": torch.empty(len(shapes[a]["file"]), dtype=torch.uint8, device="cuda"),
+            "event": torch.cuda.Event()})
+    results = torch.zeros(16 * n, dtype=torch.uint8, device="cuda")
+    cal = Calibration()
+    cal.offset.scalar = 100.0
+    cal.gain.scalar = 1.05
+
+    # The gather's copies, one per tile row of the ROI (its tiles are adjacent in the file),
+    # and its mappings: worked out once, like the reference's tile lists, and not timed.
+    for i, (a, roi) in enumerate(reqs):
+        s = slots[i]
+        tiles = shapes[a]["meta"].tiles
+        tw, th = shapes[a]["tile"]
+        across = -(-W // tw)
+        x, y, w, h = roi
+        runs, maps, at = [], [], 0
+        for r in range(y // th, (y + h - 1) // th + 1):
+            first, last = r * across + x // tw, r * across + (x + w - 1) // tw
+            b = int(tiles["offset"][first])
+            e = int(tiles["offset"][last]) + int(tiles["length"][last])
+            runs.append((b, e, at))
+            maps += [TileMapping(t, at + int(tiles["offset"][t]) - b)
+                     for t in range(first, last + 1)]
+            at += e - b
+        s["gruns"], s["gbytes"] = runs, at
+        s["gmaps"] = (TileMapping * len(maps))(*maps)
+
+    def item_for(i, mode):
+        a, roi = reqs[i]
+        s = slots[i]
+        src = CompressedInput()
+        src.metadata = shapes[a]["meta"].handle
+        if mode == "whole_archive":
+            src.bytes = ConstBytes(s["archive"].data_ptr(), len(shapes[a]["file"]))
+        elif mode == "gather":
+            src.bytes = ConstBytes(s["staging"].data_ptr(), s["gbytes"])
+            src.mappings = s["gmaps"]
+            src.mapping_count = s["need"].tiles
+        else:
+            src.bytes = ConstBytes(s["staging"].data_ptr(), s["need"].bytes)
+            src.mappings = s["maps"]
+            src.mapping_count = s["need"].tiles
+        it = BatchItem()
+        it.compressed_input = src
+        it.output = api.view(s["out"], 2, roi[2], roi[3], roi[2] * 4, s["out"].numel())
+        it.roi = Roi(*roi)
+        it.calibration = cal
+        return it
+
+    def gather(i):
+        """The reference's host gather: the ROI's tiles, row by row, into pinned staging."""
+        a, _ = reqs[i]
+        s = slots[i]
+        src = pinned[a].numpy()
+        dst = s["host_staging"].numpy()
+        for b, e, at in s["gruns"]:
+            dst[at:at + e - b] = src[b:e]
+
+    def step(mode):
+        plans = []
+        for i, (a, roi) in enumerate(reqs):
+            s = slots[i]
+            if mode == "direct":
+                st, _ = cuda.stage_roi_tiles(
+                    shapes[a]["meta"], Roi(*roi), ConstBytes(pinned[a].data_ptr(),
+                                                             len(shapes[a]["file"])),
+                    MutableBytes(s["staging"].data_ptr(), s["need"].bytes), s["maps"], copy)
+                assert st == Status.success, st
+            elif mode == "gather":
+                gather(i)
+                with torch.cuda.stream(copy):
+                    s["staging"][:s["gbytes"]].copy_(s["host_staging"][:s["gbytes"]],
+                                                     non_blocking=True)
+            else:
+                with torch.cuda.stream(copy):
+                    s["archive"].copy_(pinned[a], non_blocking=True)
+            s["event"].record(copy)
+            st, plan = cuda.prepare_batch(cuda.make_request(
+                cuda.Operation.decode_calibrate, [item_for(i, mode)]), None, prep)
+            assert st == Status.success, st
+            assert plan.workspace_bytes() <= ws.numel()
+            plans.append(plan)
+            compute.wait_event(s["event"])
+            rb = api.ResultBuffer(results.data_ptr() + 16 * i, 1)
+            assert cuda.decode_calibrate_async(plan, MutableBytes(ws.data_ptr(), ws.numel()), rb,
+                                               compute) == Status.success
+        compute.synchronize()
+        copy.synchronize()
+        return plans
+
+    need_ws = 256
+    for i in range(n):
+        for mode in ("gather", "whole_archive"):
+            st, plan = cuda.prepare_batch(cuda.make_request(cuda.Operation.decode_calibrate,
+                                                            [item_for(i, mode)]), None, prep)
+            assert st == Status.success, st
+            need_ws = max(need_ws, plan.workspace_bytes())
+    ws = torch.empty(need_ws, dtype=torch.uint8, device="cuda")
+    px = sum(r[1][2] * r[1][3] for r in reqs)
+    out = {"workload": f"{n} ROIs of the three 4096x4096 uint16 archives in pinned host memory, "
+                       "sides log-uniform 128..2048, decode_calibrate to FP32 (offset 100.0, "
+                       "gain 1.05), one plan per request",
+           "mean_roi_mpx": round(px / n / 1e6, 3)}
+    for mode in ("direct", "gather", "whole_archive"):
+        step(mode)
+        times = []
+        for _ in range(5):
+            t0 = time.perf_counter()
+            step(mode)
+            times.append(time.perf_counter() - t0)
+        sec = statistics.median(times)
+        recs = results.cpu().numpy().view(np.uint64).reshape(-1, 2)
+        assert all(int(r[0]) == 0 for r in recs), recs[:4]
+        h2d = {"direct": sum(s["need"].bytes for s in slots),
+               "gather": sum(s["gbytes"] for s in slots),
+               "whole_archive": sum(len(shapes[a]["file"]) for a, _ in reqs)}[mode]
+        out[mode] = {"ms_per_batch": round(sec * 1e3, 3), "requests_per_s": round(n / sec, 1),
+                     "decoded_gbs": round(px * 2 / sec / 1e9, 2),
+                     "h2d_mb_per_batch": round(h2d / 1e6, 2)}
+    # The outputs of the last (whole-archive) pass against a direct-staged pass.
+    keep = [s["out"].clone() for s in slots]
+    step("direct")
+    assert all(torch.equal(k, s["out"]) for k, s in zip(keep, slots)), "staged != resident"
+    out["copies_per_request"] = {
+        "direct": round(statistics.mean(s["need"].copies for s in slots), 1),
+        "gather": round(statistics.mean(len(s["gruns"]) for s in slots), 1)}
+    return out
+
+
 def run_batched(args, torch, stream, peak):
     """Config 4: 256 archives with width and height uniform in 257..4096, 70% uint16 / 30%
     float32, a random tile geometry each, decoded into pitched rows: one mixed batch (one
@@ -988,7 +1153,7 @@ def main():
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--copies", type=int, default=4)
     p.add_argument("--cpu-seconds", type=float, default=10.0)
-    p.add_argument("--sections", default="encode,calibrated,batched,serving",
+    p.add_argument("--sections", default="encode,calibrated,batched,serving,archive_roi",
                    help="extra configs reported beside the headline (comma list, or none)")
     p.add_argument("--archives", type=int, default=256, help="archives of the batched config")
     p.add_argument("--serve-archives", type=int, default=64)
@@ -1035,6 +1200,8 @@ def main():
             line["batched_decode"] = run_batched(args, torch, stream, peak)
         if "serving" in sections:
             line["serving"] = run_serving(args, torch, stream)
+        if "archive_roi" in sections:
+            line["archive_roi"] = run_archive_roi(args, torch, shapes)
         line["host_parse"] = host_parse(shapes)
         line["cpu_baseline"] = cpu_baseline(shapes, args.cpu_seconds)
         print(json.dumps(line), flush=True)

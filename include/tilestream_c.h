@@ -196,6 +196,20 @@ int ts_server_run(ts_server *server, const ts_serve_request *requests, uint64_t 
 int ts_server_pool(const ts_server *server, ts_mutable_bytes *pool);
 void ts_server_destroy(ts_server *server);
 
+/* ---- ROI staging from an archive outside the GPU (include/tilestream/staging.h) ------------
+ * No counterpart in the reference API (its benchmark gathers an ROI's tiles with host copies,
+ * benchmarks/codec_benchmark.cpp:153-320). ts_stage_roi_tiles enqueues on stream the copies of
+ * the payloads of the tiles that intersect roi, from archive (the whole .tsc file, pinned host
+ * or device memory) into staging (device memory), one copy per run of adjacent payloads (one
+ * per tile row of a parsed file; runs at most 64 KiB apart share a copy, the gap included), and
+ * writes one ts_tile_mapping per tile for a decode_roi or decode_calibrate item on a stream
+ * ordered after the copies. */
+typedef struct { uint64_t tiles, bytes, copies; } ts_roi_staging; /* RoiStaging */
+int ts_roi_staging_size(const ts_metadata *metadata, ts_roi roi, ts_roi_staging *out);
+int ts_stage_roi_tiles(const ts_metadata *metadata, ts_roi roi, ts_const_bytes archive,
+                       ts_mutable_bytes staging, ts_tile_mapping *mappings,
+                       uint64_t mapping_capacity, void *stream, ts_roi_staging *out);
+
 /* ---- allocation-free encode (no counterpart in the reference) ------------------------------
  * Encodes one image into a complete .tsc file on the GPU, like a one-item compress plan, but
  * allocates no memory: no plan tables, no workspace, no cudaMalloc or cudaFree. It is for

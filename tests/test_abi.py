@@ -45,6 +45,8 @@ CXX_SYMBOLS = [
     "tilestream::cuda::Server::seal()",            # serve.h:82
     "tilestream::cuda::Server::run(",              # serve.h:86
     "tilestream::cuda::Server::pool() const",      # serve.h:89
+    "tilestream::cuda::roi_staging_size(",         # staging.h:23
+    "tilestream::cuda::stage_roi_tiles(",          # staging.h:35
 ]
 
 

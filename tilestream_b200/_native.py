@@ -122,6 +122,10 @@ class MixedStats(C.Structure):
                 ("tuned_us", C.c_float)]
 
 
+class RoiStaging(C.Structure):
+    _fields_ = [("tiles", u64), ("bytes", u64), ("copies", u64)]
+
+
 class ServeRequest(C.Structure):
     _fields_ = [("archive", u32), ("roi", Roi), ("calibrated", u32), ("offset", C.c_float),
                 ("gain", C.c_float), ("arrival_us", C.c_double)]
@@ -180,6 +184,9 @@ _SIGNATURES = {
                                 C.POINTER(ServeStats)]),
     "ts_server_pool": (C.c_int, [vp, C.POINTER(MutableBytes)]),
     "ts_server_destroy": (None, [vp]),
+    "ts_roi_staging_size": (C.c_int, [vp, Roi, C.POINTER(RoiStaging)]),
+    "ts_stage_roi_tiles": (C.c_int, [vp, Roi, ConstBytes, MutableBytes, C.POINTER(TileMapping),
+                                     u64, vp, C.POINTER(RoiStaging)]),
     "ts_compress_noalloc": (C.c_int, [ConstImageView, TileShape, MutableBytes, vp, vp]),
     "ts_compress_noalloc_max_tiles": (u64, []),
     "ts_device_allocate": (C.c_int, [u64, vp, C.POINTER(vp)]),

@@ -4,6 +4,7 @@
 #include <tilestream/cuda.h>
 #include <tilestream/info.h>
 #include <tilestream/serve.h>
+#include <tilestream/staging.h>
 #include <tilestream_c.h>
 
 #include "plan.h"
@@ -32,6 +33,7 @@ TS_SAME_LAYOUT(ts_device_result, ts::DeviceResult);
 TS_SAME_LAYOUT(ts_parameter, ts::cuda::Parameter);
 TS_SAME_LAYOUT(ts_calibration, ts::cuda::Calibration);
 TS_SAME_LAYOUT(ts_tile_mapping, ts::cuda::TileMapping);
+TS_SAME_LAYOUT(ts_roi_staging, ts::cuda::RoiStaging);
 TS_SAME_LAYOUT(ts_parse_limits, ts::ParseLimits);
 TS_SAME_LAYOUT(ts_workspace_spec, ts::WorkspaceSpec);
 TS_SAME_LAYOUT(ts_tile_metadata, ts::TileMetadata);
@@ -420,6 +422,35 @@ extern "C" int ts_server_pool(const ts_server *server, ts_mutable_bytes *pool) {
 
 extern "C" void ts_server_destroy(ts_server *server) {
     delete server;
+}
+
+extern "C" int ts_roi_staging_size(const ts_metadata *metadata, ts_roi roi, ts_roi_staging *out) {
+    if (metadata == nullptr || out == nullptr) {
+        return code(ts::Status::invalid_argument);
+    }
+    ts::cuda::RoiStaging r;
+    const ts::Status st = ts::cuda::roi_staging_size(metadata->value, as<ts::Roi>(roi), r);
+    if (st == ts::Status::success) {
+        *out = as<ts_roi_staging>(r);
+    }
+    return code(st);
+}
+
+extern "C" int ts_stage_roi_tiles(const ts_metadata *metadata, ts_roi roi, ts_const_bytes archive,
+                                  ts_mutable_bytes staging, ts_tile_mapping *mappings,
+                                  uint64_t mapping_capacity, void *stream, ts_roi_staging *out) {
+    if (metadata == nullptr || out == nullptr) {
+        return code(ts::Status::invalid_argument);
+    }
+    ts::cuda::RoiStaging r;
+    const ts::Status st = ts::cuda::stage_roi_tiles(
+        metadata->value, as<ts::Roi>(roi), as<ts::ConstBytes>(archive),
+        as<ts::MutableBytes>(staging), reinterpret_cast<ts::cuda::TileMapping *>(mappings),
+        mapping_capacity, stream_of(stream), r);
+    if (st == ts::Status::success) {
+        *out = as<ts_roi_staging>(r);
+    }
+    return code(st);
 }
 
 // Allocation-free one-image encode (declared in include/tilestream_c.h; no counterpart in the

@@ -219,6 +219,25 @@ class Server:
             self.handle = None
 
 
+# ---- ROI staging from an archive outside the GPU (include/tilestream/staging.h) ---------------
+
+def roi_staging_size(metadata, roi):
+    """(Status, RoiStaging): the tiles, payload bytes and copies of staging `roi`."""
+    out = N.RoiStaging()
+    st = N.lib().ts_roi_staging_size(metadata.handle, roi, C.byref(out))
+    return Status(st), out
+
+
+def stage_roi_tiles(metadata, roi, archive, staging, mappings, stream=None):
+    """Enqueues the copies of the ROI's tile payloads from `archive` (ConstBytes of the whole
+    file, pinned host or device memory) into `staging` (MutableBytes of device memory) and fills
+    `mappings` (a ctypes array of TileMapping). Returns (Status, RoiStaging)."""
+    out = N.RoiStaging()
+    st = N.lib().ts_stage_roi_tiles(metadata.handle, roi, archive, staging, mappings,
+                                    len(mappings), stream_handle(stream), C.byref(out))
+    return Status(st), out
+
+
 def serve_requests(stream: dict, scale_arrivals: float = 1.0):
     """A ctypes array of ServeRequest from the arrays of workloads.serving_requests."""
     n = len(stream["arrival_us"])
