@@ -746,10 +746,13 @@ def run_archive_roi(args, torch, shapes):
         for b, e, at in s["gruns"]:
             dst[at:at + e - b] = src[b:e]
 
+    host_us = {"stage": 0.0, "prepare": 0.0, "launch": 0.0}
+
     def step(mode):
         plans = []
         for i, (a, roi) in enumerate(reqs):
             s = slots[i]
+            t0 = time.perf_counter()
             if mode == "direct":
                 st, _ = cuda.stage_roi_tiles(
                     shapes[a]["meta"], Roi(*roi), ConstBytes(pinned[a].data_ptr(),
@@ -765,15 +768,22 @@ def run_archive_roi(args, torch, shapes):
                 with torch.cuda.stream(copy):
                     s["archive"].copy_(pinned[a], non_blocking=True)
             s["event"].record(copy)
+            t1 = time.perf_counter()
             st, plan = cuda.prepare_batch(cuda.make_request(
                 cuda.Operation.decode_calibrate, [item_for(i, mode)]), None, prep)
             assert st == Status.success, st
             assert plan.workspace_bytes() <= ws.numel()
             plans.append(plan)
+            t2 = time.perf_counter()
             compute.wait_event(s["event"])
             rb = api.ResultBuffer(results.data_ptr() + 16 * i, 1)
             assert cuda.decode_calibrate_async(plan, MutableBytes(ws.data_ptr(), ws.numel()), rb,
                                                compute) == Status.success
+            t3 = time.perf_counter()
+            if mode == "direct":
+                host_us["stage"] += (t1 - t0) * 1e6
+                host_us["prepare"] += (t2 - t1) * 1e6
+                host_us["launch"] += (t3 - t2) * 1e6
         compute.synchronize()
         copy.synchronize()
         return plans
@@ -793,6 +803,8 @@ def run_archive_roi(args, torch, shapes):
            "mean_roi_mpx": round(px / n / 1e6, 3)}
     for mode in ("direct", "gather", "whole_archive"):
         step(mode)
+        for k in host_us:
+            host_us[k] = 0.0
         times = []
         for _ in range(5):
             t0 = time.perf_counter()
@@ -807,6 +819,9 @@ def run_archive_roi(args, torch, shapes):
         out[mode] = {"ms_per_batch": round(sec * 1e3, 3), "requests_per_s": round(n / sec, 1),
                      "decoded_gbs": round(px * 2 / sec / 1e9, 2),
                      "h2d_mb_per_batch": round(h2d / 1e6, 2)}
+        if mode == "direct":
+            out[mode]["host_us_per_request"] = {k: round(v / (5 * n), 1)
+                                                for k, v in host_us.items()}
     # The outputs of the last (whole-archive) pass against a direct-staged pass.
     keep = [s["out"].clone() for s in slots]
     step("direct")

@@ -653,10 +653,10 @@ bool place(std::uint64_t &total, const std::vector<T> &v, std::uint64_t &at) {
 }
 
 template <typename T>
-bool upload(void *storage, std::uint64_t at, const std::vector<T> &v, cudaStream_t stream) {
-    return v.empty() || cudaMemcpyAsync(static_cast<std::uint8_t *>(storage) + at, v.data(),
-                                        v.size() * sizeof(T), cudaMemcpyHostToDevice,
-                                        stream) == cudaSuccess;
+void pack(std::vector<std::uint8_t> &image, std::uint64_t at, const std::vector<T> &v) {
+    if (!v.empty()) {
+        std::memcpy(image.data() + at, v.data(), v.size() * sizeof(T));
+    }
 }
 
 // Kernel shape of the plain uint16 decoder (consumer warps x columns per lane, see
@@ -778,14 +778,23 @@ Status finalize(Operation operation, Draft &d, PlanState &plan, cudaStream_t str
     if (err != 0) {
         return cuda_failure("kernel preload", static_cast<cudaError_t>(err));
     }
-    if (!upload(plan.storage, at_images, d.images, stream) ||
-        !upload(plan.storage, at_tasks, d.tasks, stream) ||
-        !upload(plan.storage, at_rows, d.rows, stream) ||
-        !upload(plan.storage, at_enc, d.encode_images, stream) ||
-        !upload(plan.storage, at_cal_images, d.calib_images, stream) ||
-        !upload(plan.storage, at_cal_tasks, d.calib_tasks, stream) ||
-        cudaStreamSynchronize(stream) != cudaSuccess) {
-        return cuda_failure("plan table upload");
+    // The tables go up in one copy from one host image of the device allocation.
+    try {
+        std::vector<std::uint8_t> image(static_cast<std::size_t>(total));
+        pack(image, at_images, d.images);
+        pack(image, at_tasks, d.tasks);
+        pack(image, at_rows, d.rows);
+        pack(image, at_enc, d.encode_images);
+        pack(image, at_cal_images, d.calib_images);
+        pack(image, at_cal_tasks, d.calib_tasks);
+        if ((total != 0 && cudaMemcpyAsync(plan.storage, image.data(),
+                                           static_cast<std::size_t>(total),
+                                           cudaMemcpyHostToDevice, stream) != cudaSuccess) ||
+            cudaStreamSynchronize(stream) != cudaSuccess) {
+            return cuda_failure("plan table upload");
+        }
+    } catch (const std::bad_alloc &) {
+        return Status::resource_limit;
     }
     return Status::success;
 }

@@ -31,6 +31,7 @@
 #include "tasks.h"
 
 #include <cstdint>
+#include <mutex>
 
 namespace tsk {
 namespace {
@@ -981,17 +982,51 @@ ServeVariant select_serve(bool all_u16) {
 
 // Sets the kernel instance's shared-memory limit (which also loads it) and fills in the
 // occupancy-derived persistent grid for the plan's path mask and kernel shape.
+namespace {
+
+// What a decode plan needs of its kernel instance on a device, found by the first plan that
+// uses the instance there (which also loads it and sets its shared-memory attribute): later
+// plans skip the runtime queries. Entries are keyed by (device, kernel function).
+struct Prepared {
+    int device = -1;
+    const void *fn = nullptr;
+    int per_sm = 0;
+    int sms = 0;
+};
+constexpr int kPreparedSlots = 256;
+std::mutex g_prepared_mutex;
+Prepared g_prepared[kPreparedSlots];
+int g_prepared_count = 0;
+
+} // namespace
+
 extern "C" int tsk_decode_prepare(tsk_decode_config *config, uint32_t ntasks, int device) {
     const tsk::Variant v = tsk::select(config->paths, config->shape);
-    cudaError_t e = cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(v.smem));
-    if (e != cudaSuccess) return e;
-    int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v.fn, v.threads, v.smem);
-    if (e != cudaSuccess) return e;
-    int sms = 0;
-    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    if (e != cudaSuccess) return e;
+    const void *key = reinterpret_cast<const void *>(v.fn);
+    int per_sm = 0, sms = 0;
+    {
+        std::lock_guard<std::mutex> lock(g_prepared_mutex);
+        for (int i = 0; i < g_prepared_count; ++i) {
+            if (g_prepared[i].device == device && g_prepared[i].fn == key) {
+                per_sm = g_prepared[i].per_sm;
+                sms = g_prepared[i].sms;
+                break;
+            }
+        }
+    }
+    if (sms == 0) {
+        cudaError_t e = cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             static_cast<int>(v.smem));
+        if (e != cudaSuccess) return e;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v.fn, v.threads, v.smem);
+        if (e != cudaSuccess) return e;
+        e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        if (e != cudaSuccess) return e;
+        std::lock_guard<std::mutex> lock(g_prepared_mutex);
+        if (g_prepared_count < kPreparedSlots) {
+            g_prepared[g_prepared_count++] = {device, key, per_sm, sms};
+        }
+    }
     if (per_sm < 1) per_sm = 1;
     uint64_t grid = static_cast<uint64_t>(sms) * per_sm;
     if (grid > ntasks) grid = ntasks;
