@@ -4,9 +4,10 @@
 // with host copies into a second pinned buffer and copies that buffer to the device
 // (benchmarks/codec_benchmark.cpp:153-320). Here the copies go straight from the archive: the
 // ROI's tiles of one tile row are adjacent in a .tsc file (payloads follow the index order), so
-// one copy per tile row moves them, with no host gather; tile rows whose payloads are at most
-// 64 KiB apart go in one copy, the bytes between them included (a copy costs a few
-// microseconds of host time, in which the host link moves about 150 KB).
+// one copy per tile row moves them, with no host gather. When the archive is pinned host memory
+// or device memory, one small kernel makes all the copies of a call (it reads the archive
+// through its device address), so a call costs one launch of host time however many rows the
+// ROI spans; a pageable archive takes one cudaMemcpyAsync per row.
 #include <tilestream/cuda.h>
 
 #include <cstdint>
@@ -15,9 +16,9 @@ namespace tilestream::cuda {
 
 struct RoiStaging {
     std::uint64_t tiles = 0;  // tiles that intersect the ROI
-    std::uint64_t bytes = 0;  // bytes copied (their payloads, and any gaps copied along): the
-                              // staging buffer needs this many
-    std::uint64_t copies = 0; // copies that stage them
+    std::uint64_t bytes = 0;  // their payload bytes: the staging buffer needs this many
+    std::uint64_t copies = 0; // runs of adjacent payloads (for a parsed file, at most one
+                              // per tile row of the ROI)
 };
 
 // The tiles, bytes and copies of staging `roi` of the archive described by `metadata`.

@@ -200,10 +200,10 @@ void ts_server_destroy(ts_server *server);
  * No counterpart in the reference API (its benchmark gathers an ROI's tiles with host copies,
  * benchmarks/codec_benchmark.cpp:153-320). ts_stage_roi_tiles enqueues on stream the copies of
  * the payloads of the tiles that intersect roi, from archive (the whole .tsc file, pinned host
- * or device memory) into staging (device memory), one copy per run of adjacent payloads (one
- * per tile row of a parsed file; runs at most 64 KiB apart share a copy, the gap included), and
- * writes one ts_tile_mapping per tile for a decode_roi or decode_calibrate item on a stream
- * ordered after the copies. */
+ * or device memory) into staging (device memory), one run of adjacent payloads per tile row of
+ * a parsed file (one small kernel for all of them when the archive is pinned or on the device,
+ * one copy per run when it is pageable), and writes one ts_tile_mapping per tile for a
+ * decode_roi or decode_calibrate item on a stream ordered after the copies. */
 typedef struct { uint64_t tiles, bytes, copies; } ts_roi_staging; /* RoiStaging */
 int ts_roi_staging_size(const ts_metadata *metadata, ts_roi roi, ts_roi_staging *out);
 int ts_stage_roi_tiles(const ts_metadata *metadata, ts_roi roi, ts_const_bytes archive,

@@ -1,6 +1,7 @@
 """ROI staging on the GPU: the payloads of the tiles that intersect an ROI are copied from an
-archive in pinned host memory (or in device memory) with one copy per tile row, on a copy
-stream; the ROI is then decoded from the staged tiles on another stream. Decoded pixels must
+archive in pinned host memory, device memory or pageable host memory (one run per tile row: a
+staging kernel for the first two, one copy per run for the last), on a copy stream; the ROI is
+then decoded from the staged tiles on another stream. Decoded pixels must
 equal the crop of the source frame (reference intersecting tiles, tests/cuda_decoder_test.cpp:
 19-31; staged tiles, cuda_decoder_test.cpp:40-82)."""
 import numpy as np
@@ -70,15 +71,16 @@ def test_staged_rois_match_crop(cuda_ready, oracle_lib):
         for tile in api.TILE_SHAPES:
             file = oracle_lib.compress_image(frame, tile)
             st, meta = api.parse_metadata(np.frombuffer(file, dtype=np.uint8))
-            pinned = t.from_numpy(np.frombuffer(file, dtype=np.uint8).copy()).pin_memory()
+            pageable = np.frombuffer(file, dtype=np.uint8).copy()
+            pinned = t.from_numpy(pageable.copy()).pin_memory()
             on_device = pinned.to("cuda")
+            sources = (pinned.data_ptr(), on_device.data_ptr(), pageable.ctypes.data)
             rois = [(0, 0, 1000, 600), (999, 599, 1, 1), (tile[0] - 3, tile[1] - 2, 7, 5)]
             for _ in range(4):
                 x, y = int(rng.integers(0, 1000)), int(rng.integers(0, 600))
                 rois.append((x, y, int(rng.integers(1, 1001 - x)), int(rng.integers(1, 601 - y))))
             for k, roi in enumerate(rois):
-                src = pinned if k % 2 == 0 else on_device
-                rec, out, info = stage_and_decode(meta, src.data_ptr(), len(file), roi,
+                rec, out, info = stage_and_decode(meta, sources[k % 3], len(file), roi,
                                                   api.PixelType(ptype))
                 x, y, w, h = roi
                 want = frame[y:y + h, x:x + w]

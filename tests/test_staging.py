@@ -7,12 +7,9 @@ from tilestream_b200 import api, cuda, workloads
 from tilestream_b200.api import ConstBytes, MutableBytes, Roi, Status, TileMapping
 
 
-MERGE_GAP = 64 * 1024  # payloads at most this far apart go in one copy, the gap included
-
-
 def expected(meta, roi, tile):
     """Tiles, bytes and copies from the parsed tables: the ROI's tiles in row-major order, one
-    copy per run of payloads that follow one another, runs at most MERGE_GAP apart merged."""
+    copy per run of payloads that follow one another."""
     tiles = meta.tiles
     across = -(-meta.image.width // tile[0])
     x, y, w, h = roi
@@ -23,7 +20,7 @@ def expected(meta, roi, tile):
             t = r * across + c
             a = int(tiles["offset"][t])
             b = a + int(tiles["length"][t])
-            if end is None or a < end or a - end > MERGE_GAP:
+            if end is None or a != end:
                 if end is not None:
                     nbytes += end - begin
                 copies += 1
@@ -50,8 +47,8 @@ def test_sizes_match_tables(oracle_lib):
             assert st == Status.success
             count, nbytes, copies = expected(meta, roi, tile)
             assert (r.tiles, r.bytes, r.copies) == (count, nbytes, copies)
-            # A parsed file stores each tile row's payloads one after another: a copy covers
-            # one or more whole tile rows of the ROI.
+            # A parsed file stores each tile row's payloads one after another: at most one
+            # copy per tile row of the ROI (an ROI as wide as the image is one run).
             assert copies <= (roi[1] + roi[3] - 1) // tile[1] - roi[1] // tile[1] + 1
 
 

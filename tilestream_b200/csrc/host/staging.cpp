@@ -1,10 +1,13 @@
 // Staging the tiles of an ROI straight from an archive outside the GPU
-// (include/tilestream/staging.h). Host code only: the copies are cudaMemcpyAsync calls, one per
-// run of adjacent payloads (for a parsed file, one per tile row of the ROI), runs closer than
-// 64 KiB being merged into one copy.
+// (include/tilestream/staging.h). A copy is a run of adjacent payloads (for a parsed file, one
+// tile row of the ROI). When the archive is addressable from the device (pinned host memory,
+// device memory) and every run is 4-byte aligned, the copies are made by one small kernel
+// (kernels/stage.cu) per 160 runs; otherwise by one cudaMemcpyAsync per run.
 #include <tilestream/staging.h>
 
 #include "plan.h"
+
+#include <vector>
 
 namespace tilestream::cuda {
 namespace {
@@ -37,15 +40,10 @@ Status span_of(const ImageMetadata &m, Roi roi, Span &s) noexcept {
     return Status::success;
 }
 
-// Bytes between two runs below which they are copied as one (the gap goes along): a copy
-// costs a few microseconds of host time, in which the host link moves about 150 KB.
-constexpr std::uint64_t kMergeGap = 64 * 1024;
-
 // Calls copy(tiles, count, begin, end) for each copy, in file order: `count` tiles (their
-// indices in tiles[0 .. count)) whose payloads lie in file bytes [begin, end). A copy is a run
-// of tiles whose payloads follow one another, extended over gaps of at most kMergeGap bytes to
-// the next run. The ROI's tiles are visited in row-major order, which for a parsed file is file
-// order; tiles stored out of order start a new copy.
+// indices in tiles[0 .. count)) whose payloads lie one after another in file bytes
+// [begin, end). The ROI's tiles are visited in row-major order, which for a parsed file is
+// file order.
 template <typename Copy> void for_each_copy(const ImageMetadata &m, const Span &s, Copy copy) {
     std::uint64_t tiles[512]; // the tiles of the copy being built (flushed when full)
     std::uint64_t count = 0, begin = 0, end = 0;
@@ -53,7 +51,7 @@ template <typename Copy> void for_each_copy(const ImageMetadata &m, const Span &
         for (std::uint64_t c = s.c0; c <= s.c1; ++c) {
             const std::uint64_t t = r * s.across + c;
             const std::uint64_t a = m.tiles[t].offset, b = a + m.tiles[t].length;
-            if (count != 0 && (a < end || a - end > kMergeGap || count == 512)) {
+            if (count != 0 && (a != end || count == 512)) {
                 copy(tiles, count, begin, end);
                 count = 0;
             }
@@ -127,25 +125,71 @@ Status stage_roi_tiles(const ImageMetadata &metadata, Roi roi, ConstBytes archiv
     if (st != Status::success) {
         return st;
     }
+    // Where the device can read the archive, if it can: device memory of this device, managed
+    // memory, or host memory that is pinned (and so mapped).
+    const std::uint8_t *readable = nullptr;
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, archive.data) == cudaSuccess) {
+        if ((a.type == cudaMemoryTypeDevice && a.device == device) ||
+            a.type == cudaMemoryTypeManaged) {
+            readable = static_cast<const std::uint8_t *>(archive.data);
+        } else if (a.type == cudaMemoryTypeHost && a.devicePointer != nullptr) {
+            readable = static_cast<const std::uint8_t *>(a.devicePointer);
+        }
+    } else {
+        static_cast<void>(cudaGetLastError());
+    }
+    struct Run {
+        std::uint64_t begin, bytes, at;
+    };
+    std::vector<Run> runs;
+    try {
+        runs.reserve(static_cast<std::size_t>(need.copies));
+    } catch (...) {
+        return Status::resource_limit;
+    }
     const auto *src = static_cast<const std::uint8_t *>(archive.data);
     auto *dst = static_cast<std::uint8_t *>(staging.data);
     std::uint64_t at = 0, k = 0;
-    cudaError_t e = cudaSuccess;
+    bool words = readable != nullptr && (reinterpret_cast<std::uintptr_t>(readable) % 4) == 0 &&
+                 (reinterpret_cast<std::uintptr_t>(dst) % 4) == 0;
     for_each_copy(metadata, s,
                   [&](const std::uint64_t *tiles, std::uint64_t count, std::uint64_t begin,
                       std::uint64_t end) {
                       for (std::uint64_t i = 0; i < count; ++i) {
                           mappings[k++] = {tiles[i], at + (metadata.tiles[tiles[i]].offset - begin)};
                       }
-                      if (e == cudaSuccess) {
-                          e = cudaMemcpyAsync(dst + at, src + begin,
-                                              static_cast<std::size_t>(end - begin),
-                                              cudaMemcpyDefault, stream);
-                      }
-                      at += end - begin;
+                      const std::uint64_t bytes = end - begin;
+                      words = words && begin % 4 == 0 && bytes % 4 == 0 && at % 4 == 0 &&
+                              bytes < (1ull << 31);
+                      runs.push_back({begin, bytes, at});
+                      at += bytes;
                   });
+    cudaError_t e = cudaSuccess;
+    if (words) {
+        tsk_stage_batch batch{};
+        for (std::size_t i = 0; i < runs.size() && e == cudaSuccess; ++i) {
+            tsk_stage_run &r = batch.runs[batch.count++];
+            r.src = reinterpret_cast<std::uint64_t>(readable + runs[i].begin);
+            r.dst = reinterpret_cast<std::uint64_t>(dst + runs[i].at);
+            r.bytes = static_cast<std::uint32_t>(runs[i].bytes);
+            r.first_piece = batch.pieces;
+            batch.pieces += static_cast<std::uint32_t>((runs[i].bytes + 4095) / 4096);
+            if (batch.count == TSK_STAGE_MAX_RUNS || i + 1 == runs.size()) {
+                e = static_cast<cudaError_t>(tsk_stage_launch(&batch, stream));
+                batch = tsk_stage_batch{};
+            }
+        }
+    } else {
+        for (const Run &r : runs) {
+            if (e == cudaSuccess) {
+                e = cudaMemcpyAsync(dst + r.at, src + r.begin, static_cast<std::size_t>(r.bytes),
+                                    cudaMemcpyDefault, stream);
+            }
+        }
+    }
     if (e != cudaSuccess) {
-        return detail::cuda_failure("cudaMemcpyAsync (ROI staging)", e);
+        return detail::cuda_failure("ROI staging copies", e);
     }
     out = need;
     return Status::success;

@@ -220,6 +220,25 @@ int tsk_encode_static_launch(const tsk_encode_image *image, tsk_result *result,
                              cudaStream_t stream);
 uint64_t tsk_encode_static_max_tiles(void);
 
+// --- ROI staging: runs of bytes copied into device memory by one kernel -------------------
+
+typedef struct {
+    uint64_t src;         // device address of the run's first byte (mapped host or device memory)
+    uint64_t dst;         // device address of its destination
+    uint32_t bytes;       // a multiple of 4, as are src and dst
+    uint32_t first_piece; // 4 KiB pieces of the runs before this one
+} tsk_stage_run;
+
+// A launch's runs, passed in the kernel parameter block (under the classic 4 KB limit).
+#define TSK_STAGE_MAX_RUNS 160
+typedef struct {
+    uint32_t count;
+    uint32_t pieces; // 4 KiB pieces of all the runs
+    tsk_stage_run runs[TSK_STAGE_MAX_RUNS];
+} tsk_stage_batch;
+
+int tsk_stage_launch(const tsk_stage_batch *batch, cudaStream_t stream);
+
 int tsk_calibrate_launch(const tsk_calib_task *tasks, uint32_t ntasks,
                          const tsk_calib_image *images, uint32_t image_count, tsk_result *results,
                          cudaStream_t stream);
