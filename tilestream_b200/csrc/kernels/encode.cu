@@ -65,8 +65,10 @@ struct Divider {
 // the divisors of its copy and segment layouts.
 struct TileGeom {
     uint64_t x, y;
-    uint64_t index; // tile index within its image
+    uint64_t index;  // tile index within its image
+    uint64_t origin; // address of the tile's pixel (0, 0)
     uint32_t w, h;
+    uint32_t vector; // rows are 16-byte multiples at 16-byte-aligned addresses
     Divider vec_per_row; // 16-byte pieces per row (when rows are 16-byte multiples)
     Divider seg_per_row; // thread segments per row
 };
@@ -142,6 +144,8 @@ __device__ TileGeom tile_geom(const tsk_encode_image &im, uint64_t index) {
     g.h = static_cast<uint32_t>(im.height - g.y < im.tile_height ? im.height - g.y
                                                                  : im.tile_height);
     const uint32_t s = im.type == 2 ? 4 : 2;
+    g.origin = im.input + g.y * im.pitch + g.x * s;
+    g.vector = ((g.origin | im.pitch | (g.w * s)) & 15u) == 0;
     g.vec_per_row = Divider::of((g.w * s) / 16 != 0 ? (g.w * s) / 16 : 1);
     g.seg_per_row = Divider::of((g.w + 15) / 16);
     return g;
@@ -165,9 +169,9 @@ __device__ void issue_tile(Sh &sh, uint32_t buf, const tsk_encode_image &im, con
     constexpr uint32_t s = F32 ? 4 : 2;
     const uint32_t w = g.w, h = g.h;
     const uint32_t row_bytes = w * s;
-    const uint8_t *origin = reinterpret_cast<const uint8_t *>(im.input) + g.y * im.pitch + g.x * s;
+    const uint8_t *origin = reinterpret_cast<const uint8_t *>(g.origin);
     uint8_t *dst = reinterpret_cast<uint8_t *>(sh.raw[buf]);
-    if (((reinterpret_cast<uintptr_t>(origin) | im.pitch | row_bytes) & 15u) == 0) {
+    if (g.vector != 0) {
         const uint32_t per_row = row_bytes / 16;
         for (uint32_t c = threadIdx.x; c < h * per_row; c += kThreads) {
             const uint32_t r = g.vec_per_row.div(c), k = c - r * per_row;
@@ -652,8 +656,8 @@ __device__ void encode_chunks(Sh &sh, const Images &images, uint64_t total_tiles
     // chunk's carry; a wait that runs out marks the image's result cuda_error.
     auto settle = [&](uint32_t m, uint64_t early) {
         const LookBack lb = look_back_of(m);
-        if (lb.n == 0) {
-            return;
+        if (lb.n <= warp * 32) {
+            return; // this warp holds none of the words (warp-uniform)
         }
         bool late = false;
         uint64_t sum = 0;
