@@ -1094,6 +1094,39 @@ def run_profile_case(kind: str, launches: int = 3):
     from tilestream_b200 import api, cuda, workloads
     from tilestream_b200.api import BatchItem, CompressedInput, ConstBytes, Status, TileShape
     stream = torch.cuda.current_stream()
+    if kind == "field":
+        # Config 3's fused launch: the float32 field decoded with FP32 offset and gain maps.
+        field = workloads.field_frame(W, H, seed=3)
+        offset, gain = workloads.calibration_maps(W, H, seed=5)
+        dev_frame = torch.from_numpy(field.view(np.uint8).reshape(-1).copy()).cuda()
+        file = encode_on_gpu(torch, stream, [(dev_frame, W, H, W * 4)], 2, (128, 32))[0]
+        st, meta = api.parse_metadata(file)
+        src_dev = torch.from_numpy(np.frombuffer(file, dtype=np.uint8).copy()).cuda()
+        maps = [torch.from_numpy(m.view(np.uint8).reshape(-1).copy()).cuda()
+                for m in (offset, gain)]
+        out = torch.empty(W * H * 4, dtype=torch.uint8, device="cuda")
+        src = CompressedInput()
+        src.bytes = ConstBytes(src_dev.data_ptr(), len(file))
+        src.metadata = meta.handle
+        item = BatchItem()
+        item.compressed_input = src
+        item.output = api.view(out, 2, W, H, W * 4)
+        item.roi = api.Roi(0, 0, W, H)
+        item.calibration.offset.kind = cuda.ParameterKind.map
+        item.calibration.offset.map = api.const_view(maps[0], 2, W, H, W * 4)
+        item.calibration.gain.kind = cuda.ParameterKind.map
+        item.calibration.gain.map = api.const_view(maps[1], 2, W, H, W * 4)
+        st, plan = cuda.prepare_batch(cuda.make_request(cuda.Operation.decode_calibrate, [item]),
+                                      None, stream)
+        assert st == Status.success, st
+        ws = torch.empty(max(plan.workspace_bytes(), 256), dtype=torch.uint8, device="cuda")
+        res = torch.zeros(16, dtype=torch.uint8, device="cuda")
+        for _ in range(launches):
+            assert cuda.decode_calibrate_async(plan, ws, res, stream) == Status.success
+        torch.cuda.synchronize()
+        assert int(res.cpu().numpy().view(np.uint32)[0]) == 0
+        print(json.dumps({"profile_case": kind, "launches": launches, "images_per_launch": 1}))
+        return
     if kind == "step":
         frame, shapes, step_plans, workspace, results = prepare_workload(torch, stream, 1)
         wsb = api.MutableBytes(workspace.data_ptr(), workspace.numel())
@@ -1160,7 +1193,8 @@ def run_profile_case(kind: str, launches: int = 3):
 
 def main():
     p = argparse.ArgumentParser()
-    p.add_argument("--profile", choices=["decode", "fused", "encode", "step"], default=None,
+    p.add_argument("--profile", choices=["decode", "fused", "encode", "step", "field"],
+                   default=None,
                    help="run only a small case for ncu captures and exit")
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=3000)

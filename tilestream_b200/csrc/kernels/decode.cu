@@ -358,10 +358,39 @@ __device__ void decode_rows(const Ctx &x, const uint32_t *payload, const uint16_
             return fma_add(a, b, pipes);
         }
     };
+    // Calibration maps are read with plain loads just before each store; their lines are
+    // prefetched into L2 a row iteration ahead (and, for a task's first rows, at its start), so
+    // those loads do not wait on DRAM. Each address is one this lane reads.
+    auto prefetch_maps = [&](uint32_t row) {
+        if constexpr (Cal) {
+            if (row < x.row1) {
+                const uint64_t line = static_cast<uint64_t>(row - x.row0);
+                for (uint32_t pass = 0; pass < passes; ++pass) {
+                    const uint32_t c0 = pass * kSpan + sub * G;
+                    if (c0 < x.col1 && c0 + G > x.col0) {
+                        const uint32_t c = c0 > x.col0 ? c0 : x.col0;
+                        const uint32_t e = (c0 + G < x.col1 ? c0 + G : x.col1) - 1;
+                        if (x.omap) {
+                            const uint8_t *m = x.omap + line * x.opitch;
+                            asm volatile("prefetch.global.L2 [%0];" ::"l"(m + 4 * c));
+                            asm volatile("prefetch.global.L2 [%0];" ::"l"(m + 4 * e));
+                        }
+                        if (x.gmap) {
+                            const uint8_t *m = x.gmap + line * x.gpitch;
+                            asm volatile("prefetch.global.L2 [%0];" ::"l"(m + 4 * c));
+                            asm volatile("prefetch.global.L2 [%0];" ::"l"(m + 4 * e));
+                        }
+                    }
+                }
+            }
+        }
+    };
+    prefetch_maps(x.row0 + warp * kRowsPerWarp + lane / LW);
     for (uint32_t base = x.row0 + warp * kRowsPerWarp; base < x.row1;
          base += CW * kRowsPerWarp) {
         const uint32_t r = base + lane / LW;
         const bool live = r < x.row1;
+        prefetch_maps(r + CW * kRowsPerWarp);
         const uint64_t line_off = static_cast<uint64_t>(live ? r - x.row0 : 0u);
         uint8_t *line = x.out + line_off * x.pitch;
         const uint8_t *orow = nullptr, *grow = nullptr;
