@@ -9,12 +9,14 @@
 // The reference walks every payload twice (once to count row segments, once to fill the
 // tables). Here the index is checked first, which fixes the segment count (one per row of
 // every PREDICT tile) and where each tile's segments go, and the payloads are walked once, with
-// word loads, split over up to 8 host threads for files of at least 1024 tiles.
+// word loads, split over up to 8 host threads (TILESTREAM_PARSE_THREADS) for files of at least
+// 1024 tiles.
 #include <tilestream/api.h>
 
 #include "checked.h"
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <thread>
 #include <vector>
@@ -222,15 +224,29 @@ std::uint64_t segments_before(const std::uint8_t *d, const Header &h, std::uint6
     return nseg;
 }
 
+// Threads a parse may use: TILESTREAM_PARSE_THREADS when set (1 keeps every parse on the
+// calling thread, for processes that parse on many threads already), else up to 8 of the
+// host's cores. Read once per process.
+std::uint64_t parse_threads() noexcept {
+    static const std::uint64_t threads = [] {
+        const char *v = std::getenv("TILESTREAM_PARSE_THREADS");
+        if (v != nullptr && *v != 0) {
+            const long n = std::strtol(v, nullptr, 10);
+            return static_cast<std::uint64_t>(n < 1 ? 1 : (n > 64 ? 64 : n));
+        }
+        const unsigned cores = std::thread::hardware_concurrency();
+        return static_cast<std::uint64_t>(cores == 0 ? 1 : std::min(cores, 8u));
+    }();
+    return threads;
+}
+
 // All payloads. A large file is cut into ranges of whole tiles checked on a few host threads
 // (each range knows its first segment from the index); with fewer tiles, or when a thread
 // cannot be started, the ranges run on the calling thread. Every failure is malformed_data,
 // so it does not matter which range finds one first.
 Status check_all_payloads(const std::uint8_t *d, const Header &h, ImageMetadata *out) noexcept {
     constexpr std::uint64_t kMinTilesPerThread = 512;
-    constexpr unsigned kMostThreads = 8;
-    const unsigned cores = std::thread::hardware_concurrency();
-    std::uint64_t parts = std::min<std::uint64_t>(cores == 0 ? 1 : cores, kMostThreads);
+    std::uint64_t parts = parse_threads();
     parts = std::max<std::uint64_t>(1, std::min<std::uint64_t>(parts, h.count / kMinTilesPerThread));
     if (parts == 1) {
         return check_payloads(d, h, out, 0, h.count, 0);
