@@ -109,3 +109,21 @@ def test_staged_calibrated_roi_equals_resident_decode(cuda_ready, oracle_lib):
     assert st == Status.success and rec2[0] == 0
     assert rec == (0, roi[2] * roi[3] * 4) and rec2[2] == roi[2] * roi[3] * 4
     assert np.array_equal(out[:roi[2] * roi[3] * 4], out2[:roi[2] * roi[3] * 4])
+
+
+def test_out_of_order_payloads(cuda_ready, oracle_lib):
+    """Metadata whose tiles are stored out of file order: each tile is its own run, and the
+    staged ROI still decodes to the crop."""
+    from test_staging import permuted_archive
+    t = torch()
+    frame = workloads.detector_frame(900, 500, seed=8)
+    for tile in api.TILE_SHAPES:
+        file, meta = permuted_archive(oracle_lib, frame, tile, seed=tile[1])
+        pinned = t.from_numpy(np.frombuffer(file, dtype=np.uint8).copy()).pin_memory()
+        for roi in ((0, 0, 900, 500), (100, 40, 333, 210)):
+            rec, out, info = stage_and_decode(meta, pinned.data_ptr(), len(file), roi,
+                                              api.PixelType.uint16)
+            x, y, w, h = roi
+            want = frame[y:y + h, x:x + w]
+            assert rec == (0, want.nbytes)
+            assert np.array_equal(out.view(np.uint16).reshape(h, w), want)

@@ -75,3 +75,36 @@ def test_checks_before_any_copy(oracle_lib):
                                 maps)[0] == Status.buffer_too_small
     short = (TileMapping * (need.tiles - 1))()
     assert cuda.stage_roi_tiles(meta, roi, archive, staging, short)[0] == Status.buffer_too_small
+
+
+def permuted_archive(oracle_lib, frame, tile, seed):
+    """The file's tile payloads in a random order after its header and index, and metadata
+    (built with ImageMetadata.create) that points at the new places."""
+    file = oracle_lib.compress_image(frame, tile)
+    st, meta = api.parse_metadata(np.frombuffer(file, dtype=np.uint8))
+    assert st == Status.success
+    tiles = meta.tiles.copy()
+    start = int(tiles["offset"][0])
+    order = np.random.default_rng(seed).permutation(len(tiles))
+    out = bytearray(file[:start])
+    for t in order:
+        a, n = int(tiles["offset"][t]), int(tiles["length"][t])
+        tiles["offset"][t] = len(out)
+        out += file[a:a + n]
+    st, moved = api.ImageMetadata.create(meta.image, meta.tile, len(out), tiles,
+                                         meta.segments.copy())
+    assert st == Status.success
+    return bytes(out), moved
+
+
+def test_out_of_order_payloads_split_runs(oracle_lib):
+    """Tiles stored out of file order (possible in metadata a caller builds) start new copies;
+    the sizes still follow the tables."""
+    frame = workloads.detector_frame(900, 500, seed=8)
+    for tile in api.TILE_SHAPES:
+        _, meta = permuted_archive(oracle_lib, frame, tile, seed=tile[0])
+        for roi in ((0, 0, 900, 500), (100, 40, 333, 210)):
+            st, r = cuda.roi_staging_size(meta, Roi(*roi))
+            assert st == Status.success
+            assert (r.tiles, r.bytes, r.copies) == expected(meta, roi, tile)
+            assert r.copies > (roi[1] + roi[3] - 1) // tile[1] - roi[1] // tile[1] + 1
