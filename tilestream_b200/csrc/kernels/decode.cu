@@ -1013,9 +1013,10 @@ ServeVariant select_serve(bool all_u16) {
 // occupancy-derived persistent grid for the plan's path mask and kernel shape.
 namespace {
 
-// What a decode plan needs of its kernel instance on a device, found by the first plan that
-// uses the instance there (which also loads it and sets its shared-memory attribute): later
-// plans skip the runtime queries. Entries are keyed by (device, kernel function).
+// The occupancy of a kernel instance on a device, found by the first plan that uses the
+// instance there: later plans skip the query. Entries are keyed by (device, kernel function).
+// The shared-memory attribute is set by every plan, so a device reset cannot leave an instance
+// without it.
 struct Prepared {
     int device = -1;
     const void *fn = nullptr;
@@ -1043,10 +1044,10 @@ extern "C" int tsk_decode_prepare(tsk_decode_config *config, uint32_t ntasks, in
             }
         }
     }
+    cudaError_t e = cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(v.smem));
+    if (e != cudaSuccess) return e;
     if (sms == 0) {
-        cudaError_t e = cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             static_cast<int>(v.smem));
-        if (e != cudaSuccess) return e;
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v.fn, v.threads, v.smem);
         if (e != cudaSuccess) return e;
         e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
