@@ -859,9 +859,13 @@ extern "C" uint64_t tsk_encode_state_bytes(uint64_t total_tiles) {
 
 extern "C" int tsk_encode_prepare(int device) {
     (void)device;
-    cudaError_t e = cudaFuncSetAttribute(tsk::encode_kernel<true>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(sizeof(tsk::SharedFor<true>)));
+    // Loads every kernel a compress execution launches (the clear kernel included), so no
+    // execution has to.
+    cudaFuncAttributes attributes{};
+    cudaError_t e = cudaFuncGetAttributes(&attributes, tsk::encode_clear_kernel);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(tsk::encode_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(sizeof(tsk::SharedFor<true>)));
     if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(tsk::encode_kernel<false>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
