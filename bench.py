@@ -354,51 +354,80 @@ def run_ours(args, rank, world, device, torch, dist):
 
 def run_e2e(args, torch, stream, shapes, wsb, recs):
     """Per step: H2D copy of the three archives from pinned memory, three decodes, D2H copy of
-    the three decoded frames into pinned memory. Each archive has its own stream (with its own
-    plan, device buffers, result record and pinned buffers), so the host link carries one
-    archive's H2D while another's pixels go D2H; the timed region spans all three streams."""
+    the three decoded frames into pinned memory. Each archive alternates between two of its
+    device copies (each with its own plan, input and output buffers): its H2D copies run on
+    one stream and its decodes and D2H copies on another, ordered by events, so the host link
+    carries step i + 1's archives while step i's pixels go D2H; the timed region spans all the
+    streams."""
     from tilestream_b200 import api, cuda
     pinned_in = [torch.from_numpy(np.frombuffer(s["file"], dtype=np.uint8).copy()).pin_memory()
                  for s in shapes]
     pinned_out = [torch.empty(W * H * 2, dtype=torch.uint8).pin_memory() for _ in shapes]
-    slots = [s["copies"][k % len(s["copies"])] for k, s in enumerate(shapes)]
+    n = len(shapes)
+    h2d_streams = [torch.cuda.Stream() for _ in shapes]
     streams = [torch.cuda.Stream() for _ in shapes]
-    results = torch.zeros(16 * len(shapes), dtype=torch.uint8, device="cuda")
-    own = [api.ResultBuffer(results.data_ptr() + 16 * k, 1) for k in range(len(shapes))]
+    copied = [[torch.cuda.Event() for _ in range(2)] for _ in shapes]
+    decoded = [[torch.cuda.Event() for _ in range(2)] for _ in shapes]
+    results = torch.zeros(16 * n, dtype=torch.uint8, device="cuda")
+    own = [api.ResultBuffer(results.data_ptr() + 16 * k, 1) for k in range(n)]
+    # Each workspace is used by one stream's decodes only.
+    spaces = [torch.empty(wsb.size, dtype=torch.uint8, device="cuda") for _ in shapes]
     steps = max(3, min(args.steps, 50))
+    counter = [0]
 
-    def step():
-        for k, (s, c) in enumerate(zip(shapes, slots)):
-            with torch.cuda.stream(streams[k]):
+    def step(decode=True):
+        i = counter[0]
+        counter[0] += 1
+        slot = i % 2
+        for k, s in enumerate(shapes):
+            c = s["copies"][slot]
+            h, st_k = h2d_streams[k], streams[k]
+            if i >= 2:
+                h.wait_event(decoded[k][slot])  # the decode of step i - 2 has read this input
+            with torch.cuda.stream(h):
                 c["src"][:len(s["file"])].copy_(pinned_in[k], non_blocking=True)
-                st = cuda.decompress_async(c["plan"], wsb, own[k], streams[k])
+            copied[k][slot].record(h)
+            st_k.wait_event(copied[k][slot])
+            if decode:
+                ws = api.MutableBytes(spaces[k].data_ptr(), spaces[k].numel())
+                st = cuda.decompress_async(c["plan"], ws, own[k], st_k)
                 assert st == 0, st
+            decoded[k][slot].record(st_k)
+            with torch.cuda.stream(st_k):
                 pinned_out[k].copy_(c["out"], non_blocking=True)
 
-    def timed(n):
+    def timed(count, decode=True):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        for st in streams:
+        for st in streams + h2d_streams:
             st.wait_event(e0)
-        for _ in range(n):
-            step()
-        for st in streams:
+        for _ in range(count):
+            step(decode)
+        for st in streams + h2d_streams:
             stream.wait_stream(st)
         e1.record(stream)
         torch.cuda.synchronize()
         return e0.elapsed_time(e1)
 
-    timed(3)
+    timed(4)
     ms = timed(steps)
+    # The host link's ceiling on this box: the same copies, streams and events, no decode.
+    timed(4, decode=False)
+    link_ms = timed(steps, decode=False)
+    timed(2)  # leaves decoded outputs in the last slot for the check below
     recs_host = results.cpu().numpy().view(np.uint64).reshape(-1, 2)
     assert all(int(r[0]) == 0 and int(r[1]) == W * H * 2 for r in recs_host), recs_host
+    last = (counter[0] - 1) % 2
     for k, s in enumerate(shapes):
-        assert torch.equal(pinned_out[k], slots[k]["out"].cpu())
+        assert torch.equal(pinned_out[k], s["copies"][last]["out"].cpu())
     h2d = sum(len(s["file"]) for s in shapes)
-    d2h = 3 * W * H * 2
-    return {"value": round(3 * W * H * 2 * steps / (ms / 1e3) / 1e9, 2), "unit": "GB/s",
+    d2h = n * W * H * 2
+    return {"value": round(n * W * H * 2 * steps / (ms / 1e3) / 1e9, 2), "unit": "GB/s",
             "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "steps": steps,
-            "ms_per_step": round(ms / steps, 4), "streams": len(streams)}
+            "ms_per_step": round(ms / steps, 4), "streams": 2 * n,
+            "buffers": "two device copies per archive, alternating",
+            "copies_only_ms_per_step": round(link_ms / steps, 4),
+            "link_frac": round(link_ms / ms, 4)}
 
 
 def best_ms(fn, reps: int = 10) -> float:
