@@ -89,6 +89,19 @@ def test_every_header_and_entry_byte(oracle_lib):
                 check(oracle_lib, bytes(m))
 
 
+def test_other_format_versions_are_unsupported(oracle_lib):
+    """Only version 1.0 is defined; any other major or minor version (a v1.1 file included) is
+    unsupported, not guessed (reference docs/format.md:16-17,32)."""
+    frame = workloads.detector_frame(130, 70, seed=8)
+    file = oracle_lib.compress_image(frame)
+    assert check(oracle_lib, file) == 0
+    for major, minor in ((1, 1), (1, 0xFFFF), (2, 0), (0, 0), (0, 1)):
+        m = bytearray(file)
+        m[8:10] = major.to_bytes(2, "little")
+        m[10:12] = minor.to_bytes(2, "little")
+        assert check(oracle_lib, bytes(m)) == int(Status.unsupported_format)
+
+
 def test_seeded_mutation_campaign(oracle_lib):
     rng = np.random.default_rng(2026)
     for seed in range(13000000, 13000400):
