@@ -861,14 +861,15 @@ def run_archive_roi(args, torch, shapes):
     return out
 
 
-def run_batched(args, torch, stream, peak):
-    """Config 4: 256 archives with width and height uniform in 257..4096, 70% uint16 / 30%
-    float32, a random tile geometry each, decoded into pitched rows: one mixed batch (one
-    persistent kernel, CUDA graph, autotuned) against per-image plain decode on the same GPU."""
+def mixed_archives(torch, stream, n):
+    """The archives of config 4: n archives with width and height uniform in 257..4096, 70%
+    uint16 / 30% float32, a random tile geometry each (seed 4), encoded on the GPU and resident
+    in device memory, each with a whole-image decode item into pitched rows and its own
+    single-image plan. Returns (entries, plans, frames, keep, decoded_bytes, algorithmic
+    bytes)."""
     from tilestream_b200 import api, cuda, workloads
     from tilestream_b200.api import BatchItem, CompressedInput, ConstBytes, Status
     rng = np.random.default_rng(4)
-    n = args.archives
     dims = rng.integers(257, 4097, size=(n, 2))
     types = np.where(rng.random(n) < 0.7, 1, 2)
     shapes = [SHAPES[i] for i in rng.integers(0, 3, n)]
@@ -916,6 +917,17 @@ def run_batched(args, torch, stream, peak):
                                       None, stream)
         assert st == Status.success
         plans.append((plan, out, pitch, w, h, s))
+    return entries, plans, frames, keep, decoded_bytes, alg
+
+
+def run_batched(args, torch, stream, peak):
+    """Config 4: 256 archives with width and height uniform in 257..4096, 70% uint16 / 30%
+    float32, a random tile geometry each, decoded into pitched rows: one mixed batch (one
+    persistent kernel, CUDA graph, autotuned) against per-image plain decode on the same GPU."""
+    from tilestream_b200 import cuda
+    from tilestream_b200.api import Status
+    n = args.archives
+    entries, plans, frames, keep, decoded_bytes, alg = mixed_archives(torch, stream, n)
     results = torch.zeros(16 * n, dtype=torch.uint8, device="cuda")
     t0 = time.perf_counter()
     st, batch = cuda.prepare_mixed_batch(entries, results, stream, graph=True, autotune=True)
@@ -1118,11 +1130,85 @@ def run_serving(args, torch, stream):
 def run_profile_case(kind: str, launches: int = 3):
     """A small case for ncu captures: one launch of `kind` over four 4096x4096 frames (about
     216 MB of decode traffic, more than the 126 MB L2), repeated `launches` times; `step` is
-    the headline step itself (the three archives in one launch, about 162 MB)."""
+    the headline step itself (the three archives in one launch, about 162 MB); `field`,
+    `calibrate`, `batch` and `serve` are one launch of the fused FP32 decode, the standalone
+    calibration, the mixed batch and the serving kernel on smaller copies of their configs."""
     import torch
     from tilestream_b200 import api, cuda, workloads
     from tilestream_b200.api import BatchItem, CompressedInput, ConstBytes, Status, TileShape
     stream = torch.cuda.current_stream()
+    if kind == "calibrate":
+        # The standalone calibration kernel: a float32 4096x4096 frame with FP32 offset and gain
+        # maps (16 B per pixel, 268 MB per launch).
+        field = workloads.field_frame(W, H, seed=3)
+        offset, gain = workloads.calibration_maps(W, H, seed=5)
+        frame_dev, off_dev, gain_dev = [torch.from_numpy(a.view(np.uint8).reshape(-1).copy())
+                                        .cuda() for a in (field, offset, gain)]
+        out = torch.empty(W * H * 4, dtype=torch.uint8, device="cuda")
+        item = BatchItem()
+        item.input = api.const_view(frame_dev, 2, W, H, W * 4)
+        item.output = api.view(out, 2, W, H, W * 4)
+        item.calibration.offset.kind = cuda.ParameterKind.map
+        item.calibration.offset.map = api.const_view(off_dev, 2, W, H, W * 4)
+        item.calibration.gain.kind = cuda.ParameterKind.map
+        item.calibration.gain.map = api.const_view(gain_dev, 2, W, H, W * 4)
+        st, plan = cuda.prepare_batch(cuda.make_request(cuda.Operation.calibrate, [item]), None,
+                                      stream)
+        assert st == Status.success, st
+        res = torch.zeros(16, dtype=torch.uint8, device="cuda")
+        for _ in range(launches):
+            assert cuda.calibrate_async(plan, None, res, stream) == Status.success
+        torch.cuda.synchronize()
+        assert int(res.cpu().numpy().view(np.uint32)[0]) == 0
+        print(json.dumps({"profile_case": kind, "launches": launches, "images_per_launch": 1}))
+        return
+    if kind == "batch":
+        # Config 4's mixed batch on 48 of its archives (about 0.6 GB decoded), graph replay.
+        # The autotuner's choice is kept in the file TILESTREAM_TUNE_CACHE names, so a second
+        # run of the same command (the one under ncu) launches no trial kernels.
+        n = 48
+        entries, plans, frames, keep, decoded, alg = mixed_archives(torch, stream, n)
+        results = torch.zeros(16 * n, dtype=torch.uint8, device="cuda")
+        st, batch = cuda.prepare_mixed_batch(entries, results, stream, graph=True,
+                                             autotune=True)
+        assert st == Status.success, st
+        for _ in range(launches):
+            assert batch.run(stream) == Status.success
+        torch.cuda.synchronize()
+        assert np.all(results.cpu().numpy().view(np.uint64).reshape(-1, 2)[:, 0] == 0)
+        print(json.dumps({"profile_case": kind, "launches": launches, "images_per_launch": n,
+                          "decoded_bytes": decoded, "algorithmic_bytes": alg,
+                          **batch.stats()}))
+        return
+    if kind == "serve":
+        # Config 5's serving kernel: 4 uint16 8192x8192 archives with 64x64 tiles resident and
+        # 48 x launches requests of its ROI distribution that all arrive at once, so each launch
+        # serves 48 requests.
+        from tilestream_b200.api import ConstBytes
+        side, count = 8192, 4
+        frames = [workloads.detector_frame_torch(side, side, 5000 + k).view(torch.uint8)
+                  .reshape(-1).contiguous() for k in range(count)]
+        files = encode_on_gpu(torch, stream, [(f, side, side, side * 2) for f in frames], 1,
+                              (64, 64))
+        del frames
+        srv = cuda.Server(pool_bytes=1 << 30, max_batch=48, max_inflight=1)
+        for f in files:
+            st, meta = api.parse_metadata(f)
+            assert st == Status.success, st
+            dev = torch.from_numpy(np.frombuffer(f, dtype=np.uint8).copy()).cuda()
+            st, _ = srv.add_archive(ConstBytes(dev.data_ptr(), dev.numel()), meta, owner=dev)
+            assert st == Status.success, st
+        assert srv.seal() == Status.success
+        arrays = workloads.serving_requests(48 * launches, count, side, side, 1e12, seed=5)
+        st, outcomes, stats = srv.run(cuda.serve_requests(arrays))
+        assert st == Status.success, st
+        assert all(outcomes[i].result.status == 0 for i in range(48 * launches))
+        area = arrays["width"].astype(np.int64) * arrays["height"]
+        print(json.dumps({"profile_case": kind, "launches": stats.batches,
+                          "requests": 48 * launches, "mean_batch": round(stats.mean_batch, 2),
+                          "decoded_bytes": int((area * np.where(arrays["calibrated"], 4, 2))
+                                               .sum())}))
+        return
     if kind == "field":
         # Config 3's fused launch: the float32 field decoded with FP32 offset and gain maps.
         field = workloads.field_frame(W, H, seed=3)
@@ -1222,7 +1308,8 @@ def run_profile_case(kind: str, launches: int = 3):
 
 def main():
     p = argparse.ArgumentParser()
-    p.add_argument("--profile", choices=["decode", "fused", "encode", "step", "field"],
+    p.add_argument("--profile", choices=["decode", "fused", "encode", "step", "field",
+                                         "calibrate", "batch", "serve"],
                    default=None,
                    help="run only a small case for ncu captures and exit")
     p.add_argument("--gpus", type=int, default=1)
