@@ -138,13 +138,13 @@ __device__ __forceinline__ uint32_t unzig16(uint32_t w, uint32_t m, uint32_t mh)
     return (h & mh) ^ sign;
 }
 
-// uint16 rows (b <= 16): the 64-bit window of the packed words that starts at the bit of item
-// `first` (item c holds residual c - 1). Item 0 starts b bits before the packed words, inside
-// the row descriptor's width word, whose top 16 bits are zero in every accepted file (the
-// reserved bytes are zero and b <= 16): item 0 therefore reads as zero, and the seed enters as
-// the scan's initial carry.
-__device__ __forceinline__ void window16(const uint32_t *packed, uint32_t first, uint32_t b,
-                                         uint32_t &x0, uint32_t &x1) {
+// The 64-bit window of the packed words that starts at the bit of item `first` of a row (item c
+// holds residual c - 1; the seed enters as the scan's initial carry). Item 0 starts b bits
+// before the packed words, inside the row descriptor's width word, whose bits 8..31 are its
+// reserved bytes, zero in every accepted file: for b <= 24 (every uint16 row) item 0 reads as
+// zero; wider FP32 rows reach the width byte, so their caller clears item 0.
+__device__ __forceinline__ void window(const uint32_t *packed, uint32_t first, uint32_t b,
+                                       uint32_t &x0, uint32_t &x1) {
     const int32_t pos = static_cast<int32_t>(first * b) - static_cast<int32_t>(b);
     const int32_t q = pos >> 5; // -1 for item 0
     const uint32_t s = static_cast<uint32_t>(pos) & 31u;
@@ -165,23 +165,6 @@ __device__ __forceinline__ void keep_bits(uint32_t &x0, uint32_t &x1, uint32_t n
     }
 }
 
-// The 64-bit window of the packed words that starts at the bit of item `first` of a row: item
-// c holds residual c - 1, item 0 holds zero (the seed is the scan's initial carry).
-__device__ __forceinline__ void window(const uint32_t *packed, uint32_t first, uint32_t b,
-                                       uint32_t &x0, uint32_t &x1) {
-    const int32_t pos = static_cast<int32_t>(first * b) - static_cast<int32_t>(b);
-    const uint32_t p = pos < 0 ? 0u : static_cast<uint32_t>(pos);
-    const uint32_t q = p >> 5, s = p & 31u;
-    const uint32_t w0 = packed[q], w1 = packed[q + 1], w2 = packed[q + 2];
-    x0 = __funnelshift_r(w0, w1, s);
-    x1 = __funnelshift_r(w1, w2, s);
-    if (pos < 0) {
-        // Item 0 of the row: shift a zero item in front of residual 0.
-        x1 = __funnelshift_lc(x0, x1, b);
-        x0 = __funnelshift_lc(0u, x0, b);
-    }
-}
-
 // G scan terms of one lane: columns [c0, c0 + G) of a row of width w with residual width b.
 // Partial: the group may run past the end of the row (those items become zero).
 template <uint32_t G, bool F32, bool Partial>
@@ -196,7 +179,7 @@ __device__ __forceinline__ void terms(const uint32_t *packed, uint32_t c0, uint3
 #pragma unroll
         for (uint32_t q = 0; q < G; q += 4) {
             uint32_t x0, x1;
-            window16(packed, c0 + q, b, x0, x1);
+            window(packed, c0 + q, b, x0, x1);
             if constexpr (Partial) {
                 if (c0 + q + 4 > w) {
                     const uint32_t items = w > c0 + q ? w - (c0 + q) : 0u;
@@ -226,6 +209,9 @@ __device__ __forceinline__ void terms(const uint32_t *packed, uint32_t c0, uint3
             }
             t[q] = x0 & m;
             t[q + 1] = __funnelshift_rc(x0, x1, b) & m;
+        }
+        if (c0 == 0) {
+            t[0] = 0; // item 0 (see window)
         }
     }
 }
