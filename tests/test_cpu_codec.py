@@ -77,6 +77,37 @@ def test_field_frame_special_words(oracle_lib):
                                                        frame)
 
 
+def _dataset_fixtures():
+    path = os.path.join(oracle.REFERENCE_DIR, "datasets", "fixtures")
+    if not os.path.isdir(path):
+        pytest.skip("reference dataset fixtures not present")
+    for name in sorted(os.listdir(path)):
+        if name.endswith(".npy"):
+            yield name, np.load(os.path.join(path, name), allow_pickle=False)
+
+
+def test_dataset_fixtures_match_reference(oracle_lib, reference):
+    """The reference's committed image fixtures (datasets/fixtures/*.npy: a CT slice, an
+    elevation field and two generated images, read in place): for every tile shape the library's
+    encoder, the oracle and the reference build emit the same bytes, and the file decodes back
+    to the same words."""
+    seen = 0
+    for name, img in _dataset_fixtures():
+        assert img.ndim == 2 and img.dtype in (np.uint16, np.float32), name
+        words = np.ascontiguousarray(img if img.dtype == np.uint16 else img.view(np.uint32))
+        ptype = 1 if words.dtype == np.uint16 else 2
+        h, w = words.shape
+        for tile in api.TILE_SHAPES:
+            file = encode(words, ptype, w, h, w * words.itemsize, tile)
+            assert file == oracle_lib.compress_image(words, tile), (name, tile)
+            assert file == reference.compress_image(words, tile), (name, tile)
+            st, out = decode(file, ptype, w, h)
+            assert st == Status.success, (name, tile)
+            assert np.array_equal(out.view(words.dtype).reshape(h, w), words), (name, tile)
+        seen += 1
+    assert seen >= 2
+
+
 def test_every_uint16_value(oracle_lib):
     img = np.arange(65536, dtype=np.uint16).reshape(256, 256)[:, ::-1].copy()
     file = encode(img, 1, 256, 256, 512)
