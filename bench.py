@@ -1132,7 +1132,8 @@ def run_profile_case(kind: str, launches: int = 3):
     216 MB of decode traffic, more than the 126 MB L2), repeated `launches` times; `step` is
     the headline step itself (the three archives in one launch, about 162 MB); `field`,
     `calibrate`, `batch` and `serve` are one launch of the fused FP32 decode, the standalone
-    calibration, the mixed batch and the serving kernel on smaller copies of their configs."""
+    calibration, the mixed batch and the serving kernel on smaller copies of their configs;
+    `stage` stages one ROI's payloads from pinned host memory."""
     import torch
     from tilestream_b200 import api, cuda, workloads
     from tilestream_b200.api import BatchItem, CompressedInput, ConstBytes, Status, TileShape
@@ -1209,6 +1210,37 @@ def run_profile_case(kind: str, launches: int = 3):
                           "decoded_bytes": int((area * np.where(arrays["calibrated"], 4, 2))
                                                .sum())}))
         return
+    if kind == "stage":
+        # The ROI staging kernel: the payloads of a 2048x2048 ROI (64 tile rows of 16 tiles, one
+        # run each) of the seed-2 frame's 128x32 archive, read from pinned host memory.
+        from tilestream_b200.api import MutableBytes, Roi, TileMapping
+        frame = workloads.detector_frame(W, H, seed=SEED)
+        dev_frame = torch.from_numpy(frame.view(np.uint8).reshape(-1).copy()).cuda()
+        file = encode_on_gpu(torch, stream, [(dev_frame, W, H, W * 2)], 1, (128, 32))[0]
+        del dev_frame
+        st, meta = api.parse_metadata(file)
+        assert st == Status.success, st
+        pinned = torch.from_numpy(np.frombuffer(file, dtype=np.uint8).copy()).pin_memory()
+        roi = Roi(1024, 1024, 2048, 2048)
+        st, need = cuda.roi_staging_size(meta, roi)
+        assert st == Status.success, st
+        staging = torch.empty(need.bytes, dtype=torch.uint8, device="cuda")
+        maps = (TileMapping * need.tiles)()
+        for _ in range(launches):
+            st, got = cuda.stage_roi_tiles(meta, roi, ConstBytes(pinned.data_ptr(), len(file)),
+                                           MutableBytes(staging.data_ptr(), need.bytes), maps,
+                                           stream)
+            assert st == Status.success, st
+        torch.cuda.synchronize()
+        host = staging.cpu().numpy()
+        tiles = meta.tiles
+        for m in maps:
+            t = int(m.tile_index)
+            a, n = int(tiles["offset"][t]), int(tiles["length"][t])
+            assert host[m.input_offset:m.input_offset + n].tobytes() == file[a:a + n]
+        print(json.dumps({"profile_case": kind, "launches": launches, "tiles": need.tiles,
+                          "bytes": need.bytes, "copies": need.copies}))
+        return
     if kind == "field":
         # Config 3's fused launch: the float32 field decoded with FP32 offset and gain maps.
         field = workloads.field_frame(W, H, seed=3)
@@ -1270,8 +1302,9 @@ def run_profile_case(kind: str, launches: int = 3):
                                       stream)
         executor = cuda.compress_async
     else:
-        import oracle
-        file = oracle.Oracle().compress_image(frame, (128, 32))
+        dev_frame = torch.from_numpy(frame.view(np.uint8).reshape(-1).copy()).cuda()
+        file = encode_on_gpu(torch, stream, [(dev_frame, W, H, W * 2)], 1, (128, 32))[0]
+        del dev_frame
         st, meta = api.parse_metadata(file)
         items, keep = [], [meta]
         for _ in range(4):
@@ -1309,7 +1342,7 @@ def run_profile_case(kind: str, launches: int = 3):
 def main():
     p = argparse.ArgumentParser()
     p.add_argument("--profile", choices=["decode", "fused", "encode", "step", "field",
-                                         "calibrate", "batch", "serve"],
+                                         "calibrate", "batch", "serve", "stage"],
                    default=None,
                    help="run only a small case for ncu captures and exit")
     p.add_argument("--gpus", type=int, default=1)
