@@ -1049,6 +1049,61 @@ def serve_summary(stats, count):
             "max_inflight": stats.max_inflight, "stalls": stats.stalls, "tiles": stats.tiles}
 
 
+class _DeviceBytes:
+    """A view of device memory that the library owns (a server's output pool) for torch."""
+
+    def __init__(self, address: int, nbytes: int):
+        self.__cuda_array_interface__ = {"shape": (nbytes,), "typestr": "|u1",
+                                         "data": (address, False), "version": 3}
+
+
+def serving_calibration_error(torch, n, side, rate, resident, metas):
+    """Served FP32 calibrated outputs against FP64 and against the host two-rounding form
+    (x - offset, then times gain, each rounded to binary32): the calibrated requests among 200
+    of the serving distribution (seed 8), outputs kept in the pool and read back."""
+    from tilestream_b200 import cuda, workloads
+    from tilestream_b200.api import ConstBytes, Status
+    arrays = workloads.serving_requests(200, n, side, side, rate, seed=8)
+    keep = np.flatnonzero(arrays["calibrated"])
+    arrays = {k: v[keep] for k, v in arrays.items()}
+    w, h = arrays["width"].astype(np.int64), arrays["height"].astype(np.int64)
+    need = int((((w * 4 + 15) // 16 * 16 * h + 255) // 256 * 256).sum())
+    srv = cuda.Server(pool_bytes=need, max_batch=48, max_inflight=4, retain_outputs=True)
+    for dev, meta in zip(resident, metas):
+        st, _ = srv.add_archive(ConstBytes(dev.data_ptr(), dev.numel()), meta, owner=dev)
+        assert st == Status.success, st
+    assert srv.seal() == Status.success
+    st, outcomes, _ = srv.run(cuda.serve_requests(arrays))
+    assert st == Status.success, st
+    torch.cuda.synchronize()
+    p = srv.pool()
+    pool = torch.as_tensor(_DeviceBytes(p.data, need), device="cuda")
+    worst, same, pixels, frame, current = 0.0, True, 0, None, -1
+    for i in np.argsort(arrays["archive"], kind="stable"):  # one source frame at a time
+        oc = outcomes[int(i)]
+        assert oc.result.status == 0, (i, oc.result.status)
+        a = int(arrays["archive"][i])
+        if a != current:
+            frame, current = workloads.detector_frame_torch(side, side, 5000 + a), a
+        x0, y0, rw, rh = (int(arrays[k][i]) for k in ("x", "y", "width", "height"))
+        x = frame[y0:y0 + rh, x0:x0 + rw].cpu().numpy().astype(np.float32)
+        rows = pool[oc.output_offset:oc.output_offset + oc.output_pitch * rh].view(rh, -1)
+        got = rows[:, :rw * 4].contiguous().view(torch.float32).cpu().numpy()
+        o, g = np.float32(arrays["offset"][i]), np.float32(arrays["gain"][i])
+        host_form = ((x - o).astype(np.float32) * g).astype(np.float32)
+        same = same and bool(np.array_equal(got.view(np.uint32), host_form.view(np.uint32)))
+        ref = (x.astype(np.float64) - float(o)) * float(g)
+        normal = np.abs(ref) >= 2.0 ** -126
+        ulp = np.spacing(np.abs(ref[normal]).astype(np.float32)).astype(np.float64)
+        if ulp.size:
+            worst = max(worst, float(np.max(np.abs(got[normal] - ref[normal]) / ulp)))
+        pixels += rw * rh
+    del srv
+    return {"requests": int(len(keep)), "pixels": int(pixels),
+            "equals_host_two_rounding_form": same,
+            "max_ulp_vs_fp64_normal_results": round(worst, 4), "ulp_bound": 1.5}
+
+
 def run_serving(args, torch, stream):
     """Config 5: 64 uint16 8192x8192 archives with 64x64 tiles resident in device memory; a
     request stream with Poisson arrivals at 20k req/s, each an ROI with sides log-uniform in
@@ -1111,6 +1166,8 @@ def run_serving(args, torch, stream):
         sweep.append(point)
     results["rate_sweep"] = sweep
     servers.clear()
+    results["calibration_error"] = serving_calibration_error(torch, n, side, rate, resident,
+                                                             metas)
     area = stream_arrays["width"].astype(np.float64) * stream_arrays["height"]
     return {"workload": f"{n} uint16 {side}x{side} archives, 64x64 tiles, resident; Poisson "
                         f"arrivals at {rate:.0f} req/s; ROI sides log-uniform 32..4096 at a "
