@@ -10,11 +10,18 @@ own golden file byte for byte.
 It also records the C1 golden round trip (uint16 1024x1024 frame, seed 1, tiles 128x32): the
 SHA-256 and size of the reference encoding, in c1_roundtrip.json.
 
+And it extracts the reference's calibration contract rows (tests/numerics/support.h:404-456:
+special-value inputs with their exact expected words, which the reference runs through its host
+form and every GPU calibration path, tests/numerics_test.cpp:79-87,
+tests/cuda_numerics_test.cpp:161-200) into calibration_contract_rows.json, after checking that
+the oracle's host form reproduces each of them.
+
 Run from the repository root:  python tests/golden/make_golden.py
 """
 import hashlib
 import json
 import os
+import re
 import sys
 
 import numpy as np
@@ -58,7 +65,36 @@ def read_hex(path: str) -> bytes:
         return bytes(int(tok, 16) for tok in f.read().split())
 
 
+def contract_rows():
+    """The rows of the reference's contract_rows[] table, read from its header text."""
+    with open(os.path.join(oracle.REFERENCE_DIR, "tests", "numerics", "support.h")) as f:
+        text = f.read()
+    block = text[text.index("contract_rows[] = {"):]
+    block = block[:block.index("};")]
+    word = r"(0x[0-9a-fA-F]{8})"
+    rows = re.findall(r"\{" + ", ".join([word] * 4) + r', "([^"]*)"\}', block)
+    assert len(rows) == block.count('"') // 2, "a row did not parse"
+    return [{"x": x, "offset": o, "gain": g, "expected": e, "note": n}
+            for x, o, g, e, n in rows]
+
+
+def same_word(got: int, want: int) -> bool:
+    """Equal words, or both NaN (the contract compares NaNs by class)."""
+    nan = lambda w: (w & 0x7f800000) == 0x7f800000 and (w & 0x007fffff) != 0  # noqa: E731
+    return got == want or (nan(got) and nan(want))
+
+
 def main():
+    rows = contract_rows()
+    words = lambda key: np.array([[int(r[key], 16) for r in rows]], np.uint32)  # noqa: E731
+    got = oracle.Oracle().calibrate_image(words("x"), words("offset").view(np.float32),
+                                          words("gain").view(np.float32)).view(np.uint32)[0]
+    for r, g in zip(rows, got):
+        assert same_word(int(g), int(r["expected"], 16)), (r["note"], hex(int(g)))
+    with open(os.path.join(HERE, "calibration_contract_rows.json"), "w") as f:
+        json.dump(rows, f, indent=1)
+        f.write("\n")
+
     ref = oracle.Reference()
     manifest = {}
     for name, w, h, pixels, mode in cases():

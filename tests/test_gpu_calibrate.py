@@ -3,6 +3,9 @@ Standalone and fused results must equal the host two-rounding form bit for bit e
 payloads, equal each other bit for bit (NaNs included), and stay within 1.5 ulp of the FP64
 reference for normal results (reference tests/cuda_calibration_test.cpp:121-135,208,328-389,
 tests/numerics/support.h:52-57)."""
+import json
+import os
+
 import numpy as np
 import pytest
 
@@ -135,3 +138,75 @@ def test_fused_equals_separate(cuda_ready, oracle_lib, ptype):
             region = frame[y:y + h, x:x + w]
             separate = gpu_calibrate(region, off, np.float32(1.05) if roi[0] else gain)
             assert np.array_equal(fused, separate), (tile, roi)
+
+
+def contract_rows():
+    with open(os.path.join(os.path.dirname(__file__), "golden",
+                           "calibration_contract_rows.json")) as f:
+        return json.load(f)
+
+
+def fused(oracle_lib, samples, offset, gain):
+    """decode_calibrate of a one-row archive of `samples` with per-pixel maps."""
+    h, w = samples.shape
+    src, meta, dev = parsed_source(oracle_lib.compress_image(samples))
+    keep = [meta, dev]
+    cal = calibration(offset, gain, keep)
+    out = device_bytes(w * h * 4)
+    keep.append(out)
+    item = decode_item(src, 2, out, w, h, w * 4, (0, 0, w, h), cal)
+    run = Run(cuda.Operation.decode_calibrate, [item], keep=keep)
+    assert run.status == Status.success
+    assert run.execute(cuda.decode_calibrate_async) == Status.success
+    assert run.records()[0] == (0, 0, w * h * 4)
+    return host(out).view(np.uint32).reshape(h, w)
+
+
+def test_special_value_contract(cuda_ready, oracle_lib):
+    """The reference's 42 special-value contract rows with their exact expected words
+    (tests/numerics/support.h:404-456; NaN results compare by class), through every path the
+    reference runs them on (tests/cuda_numerics_test.cpp:161-200): per-pixel maps standalone
+    and fused, the rows whose sample is a uint16 value as uint16 samples standalone and fused,
+    and one 1x1 image per row with scalar parameters."""
+    rows = contract_rows()
+    word = lambda key, sel=rows: np.array([[int(r[key], 16) for r in sel]],  # noqa: E731
+                                          np.uint32)
+    as_f32 = lambda a: a.view(np.float32)  # noqa: E731
+
+    def check(got, sel, path):
+        want = word("expected", sel)
+        assert np.all(same_bits_or_both_nan(got, want)), (
+            path, [r["note"] for r, ok in zip(sel, same_bits_or_both_nan(got, want)[0]) if not ok])
+
+    x, o, g = word("x"), as_f32(word("offset")), as_f32(word("gain"))
+    check(gpu_calibrate(x, o, g), rows, "maps")
+    check(fused(oracle_lib, x, o, g), rows, "fused")
+
+    def is_uint16(r):
+        v = np.uint32(int(r["x"], 16)).view(np.float32)
+        return bool(0 <= v <= 65535 and v == np.floor(v) and not np.signbit(v))
+
+    ints = [r for r in rows if is_uint16(r)]
+    assert len(ints) >= 10
+    xi = as_f32(word("x", ints)).astype(np.uint16)
+    oi, gi = as_f32(word("offset", ints)), as_f32(word("gain", ints))
+    check(gpu_calibrate(xi, oi, gi), ints, "uint16")
+    check(fused(oracle_lib, xi, oi, gi), ints, "uint16 fused")
+
+    items, outs, keep = [], [], []
+    for r in rows:
+        inp = to_device(np.array([int(r["x"], 16)], np.uint32).view(np.uint8))
+        out = device_bytes(4)
+        outs.append(out)
+        keep += [inp, out]
+        item = BatchItem()
+        item.input = api.const_view(inp, 2, 1, 1, 4, 4)
+        item.output = api.view(out, 2, 1, 1, 4, 4)
+        item.calibration = calibration(np.uint32(int(r["offset"], 16)).view(np.float32),
+                                       np.uint32(int(r["gain"], 16)).view(np.float32), keep)
+        items.append(item)
+    run = Run(cuda.Operation.calibrate, items, keep=keep)
+    assert run.status == Status.success
+    assert run.execute(cuda.calibrate_async) == Status.success
+    assert all(rec == (0, 0, 4) for rec in run.records())
+    check(np.array([[host(out).view(np.uint32)[0] for out in outs]]), rows, "scalars")

@@ -51,6 +51,43 @@ def test_golden_files_match_reference_checkout():
         assert read_hex(name) == upstream, name
 
 
+def contract_rows():
+    with open(os.path.join(GOLDEN, "calibration_contract_rows.json")) as f:
+        return json.load(f)
+
+
+def same_word(got, want):
+    """Equal words, or both NaN (NaN results compare by class)."""
+    nan = lambda w: (w & 0x7f800000) == 0x7f800000 and (w & 0x007fffff) != 0  # noqa: E731
+    return got == want or (nan(got) and nan(want))
+
+
+def test_calibration_contract_rows(oracle_lib):
+    """The reference's special-value contract (tests/numerics/support.h:404-456, run on the host
+    form by tests/numerics_test.cpp:79-87): the oracle's two-rounding form gives each row's
+    exact word."""
+    rows = contract_rows()
+    assert len(rows) == 42
+    words = lambda k: np.array([[int(r[k], 16) for r in rows]], np.uint32)  # noqa: E731
+    got = oracle_lib.calibrate_image(words("x"), words("offset").view(np.float32),
+                                     words("gain").view(np.float32)).view(np.uint32)[0]
+    for r, g in zip(rows, got):
+        assert same_word(int(g), int(r["expected"], 16)), (r["note"], hex(int(g)))
+
+
+def test_calibration_contract_rows_match_reference_checkout():
+    """The committed rows equal the reference header's table (when present)."""
+    path = os.path.join(oracle.REFERENCE_DIR, "tests", "numerics", "support.h")
+    if not os.path.exists(path):
+        pytest.skip("reference checkout not present")
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(
+        "make_golden", os.path.join(GOLDEN, "make_golden.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    assert mod.contract_rows() == contract_rows()
+
+
 def test_format_worked_example(oracle_lib):
     """docs/format.md:77: three 3-bit residuals [1, 2, 7] pack to the word 0x000001d1. A row
     100, 99, 100, 96, 96, ... has deltas -1, +1, -4 (zigzag 1, 2, 7) followed by zeros."""
