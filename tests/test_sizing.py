@@ -46,3 +46,19 @@ def test_workspace_size_matches_reference(reference):
         assert int(st) == want[0], (i, k, tile, temp)
         if want[0] == 0:
             assert got == want[1], (i, k, tile, temp)
+
+
+def test_documented_examples():
+    """The reference's worked examples, independent of the reference build: compress_bound of
+    a 1x1 image of either type is 100 B, of a 128x32 uint16 image 8288 B and of 129x33 8708 B
+    (docs/format.md:132); the fixed workspace regions for one default tile and one image total
+    17664 B, with A256(S) appended, and the empty spec needs zero bytes (docs/api.md:107)."""
+    for ptype, w, h, want in ((1, 1, 1, 100), (2, 1, 1, 100), (1, 128, 32, 8288),
+                              (1, 129, 33, 8708)):
+        st, got = api.compress_bound(ImageSpec(ptype, w, h), TileShape())
+        assert int(st) == 0 and got == want, (ptype, w, h)
+    for temp, want in ((0, 17664), (1, 17664 + 256), (256, 17664 + 256), (257, 17664 + 512)):
+        st, got = api.workspace_size(WorkspaceSpec(1, 1, TileShape(128, 32), temp))
+        assert int(st) == 0 and got == want, temp
+    st, got = api.workspace_size(WorkspaceSpec(0, 0, TileShape(128, 32), 0))
+    assert int(st) == 0 and got == 0
