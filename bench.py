@@ -1169,7 +1169,7 @@ def serving_calibration_error(torch, n, side, rate, resident, metas):
             worst = max(worst, float(np.max(np.abs(got[normal] - ref[normal]) / ulp)))
         contract = merge_contract(contract, calibration_contract(x, o, g, got))
         pixels += rw * rh
-    del srv
+    del pool, srv  # the view first: the pool's memory belongs to the server
     return {"requests": int(len(keep)), "pixels": int(pixels),
             "equals_host_two_rounding_form": same,
             "max_ulp_vs_fp64_normal_results": round(worst, 4), "ulp_bound": 1.5,
