@@ -1,6 +1,6 @@
 // Thin inline-PTX wrappers for the sm_90+/sm_100a asynchronous data movement used by the
 // kernels: mbarrier phases, the bulk (TMA engine) global->shared copy, and 4-byte cp.async.
-// No multicast form is used anywhere.
+// Every copy has exactly one destination CTA: this one.
 #pragma once
 
 #include <cstdint>
