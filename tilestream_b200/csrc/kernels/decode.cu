@@ -925,8 +925,10 @@ Variant make() {
 // Shapes of the plain uint16 instance (consumer warps x uint16 columns per lane, stages,
 // resident CTAs per SM): 0 = 8 x 8, 4 stages, 4; 1 = 8 x 16, 4, 3; 2 = 4 x 16, 4, 5;
 // 3 = 4 x 8, 4, 6; 4 = 4 x 16, 4, 6 (64 registers); 5 = 4 x 16, 3, 7 (56 registers);
-// 6 = 4 x 32, 4, 3; 7 = 4 x 32, 4, 4. The other instances have shapes 0 and 2 (odd shapes map
-// to 0, even ones to 2).
+// 6 = 4 x 32, 4, 3; 7 = 4 x 32, 4, 4. The plain mixed uint16 + FP32 instance has four: 0 =
+// 8 x 8, 3 stages of 16 KiB, 3 CTAs; 1 = 4 x 16, 2 stages, 5 CTAs; 2 = 4 x 16, 3, 4; 3 = 4 x 8,
+// 2, 6 (two stages leave shared memory for more resident CTAs). The other instances have shapes
+// 0 and 2 (odd shapes map to 0, even ones to 2).
 Variant select(uint32_t paths, uint32_t shape) {
     const bool f32 = paths & kF32, u16 = paths & kU16, plain = paths & kPlain, c = paths & kCal;
     const bool narrow = shape % 2 == 0 && shape != 0; // four consumer warps
@@ -966,8 +968,15 @@ Variant select(uint32_t paths, uint32_t shape) {
         }
     } else if (plain && !c) {
         // Mixed uint16 and FP32 archives, plain decode (no calibrated code in the instance).
-        return narrow ? make<16384, 3, kU16 | kF32 | kPlain, 4, 16, 4>()
-                      : make<16384, 3, kU16 | kF32 | kPlain>();
+        switch (shape) {
+        case 1:
+            return make<16384, 2, kU16 | kF32 | kPlain, 4, 16, 5>();
+        case 3:
+            return make<16384, 2, kU16 | kF32 | kPlain, 4, 8, 6>();
+        default:
+            return narrow ? make<16384, 3, kU16 | kF32 | kPlain, 4, 16, 4>()
+                          : make<16384, 3, kU16 | kF32 | kPlain>();
+        }
     }
     return narrow ? make<16384, 3, kU16 | kF32 | kPlain | kCal, 4, 16, 4>()
                   : make<16384, 3, kU16 | kF32 | kPlain | kCal>();
