@@ -224,8 +224,9 @@ int ts_stage_roi_tiles(const ts_metadata *metadata, ts_roi roi, ts_const_bytes a
  * input, output and result are device memory of the current device; output needs
  * compress_bound bytes and result one ts_device_result. Arguments are checked as for
  * compress_async, statuses are the same, and per-image completion is written to *result.
- * The first call on each device sets up that device's scratch address and must therefore
- * come before any stream capture on it. Every call shares the array and clears what it uses:
+ * The first call on each device loads the kernels there and sizes their grid, and must
+ * therefore come before any stream capture on that device; every call looks up the device's
+ * address of the array afresh. Every call shares the array and clears what it uses:
  * calls that overlap on one GPU race, so order them on one stream or with events. */
 int ts_compress_noalloc(ts_const_image_view input, ts_tile_shape tile, ts_mutable_bytes output,
                         ts_device_result *result, void *stream);

@@ -19,7 +19,13 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libtsref.so")
-REFERENCE_DIR = "/root/reference"
+
+def reference_dir() -> str | None:
+    """The reference checkout named by the TILESTREAM_REFERENCE environment variable, when that
+    names a directory; None otherwise (no path is assumed)."""
+    path = os.environ.get("TILESTREAM_REFERENCE")
+    return path if path and os.path.isdir(path) else None
+
 
 UINT16, FLOAT32 = 1, 2
 RAW, CONSTANT, PREDICT = 0, 1, 2
@@ -48,10 +54,12 @@ class Limits(C.Structure):
 
 
 def build(reference: bool = True) -> None:
-    """Compiles liboracle.so, and oracle/_ref when the reference checkout is present."""
+    """Compiles liboracle.so, and oracle/_ref when TILESTREAM_REFERENCE names the reference
+    checkout (an already built oracle/_ref is kept otherwise)."""
     subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
-    if reference and os.path.isdir(os.path.join(REFERENCE_DIR, "src", "cpu")):
-        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={REFERENCE_DIR}"], check=True)
+    ref = reference_dir()
+    if reference and ref and os.path.isdir(os.path.join(ref, "src", "cpu")):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={ref}"], check=True)
 
 
 def _ptr(a) -> C.c_void_p:

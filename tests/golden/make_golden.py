@@ -16,12 +16,19 @@ form and every GPU calibration path, tests/numerics_test.cpp:79-87,
 tests/cuda_numerics_test.cpp:161-200) into calibration_contract_rows.json, after checking that
 the oracle's host form reproduces each of them.
 
-Run from the repository root:  python tests/golden/make_golden.py
+And it copies the reference's committed test inputs that the GPU parity tests replay, so that
+no test needs the reference checkout at run time: the two fuzz corpora (fuzz/corpus/parse and
+fuzz/corpus/mutation, every file) into fuzz_corpus.npz, and the four image fixtures
+(datasets/fixtures/*.npy) into datasets/.
+
+Run from the repository root, with TILESTREAM_REFERENCE naming the reference checkout:
+    TILESTREAM_REFERENCE=<checkout> python tests/golden/make_golden.py
 """
 import hashlib
 import json
 import os
 import re
+import shutil
 import sys
 
 import numpy as np
@@ -65,9 +72,33 @@ def read_hex(path: str) -> bytes:
         return bytes(int(tok, 16) for tok in f.read().split())
 
 
+def reference_checkout() -> str:
+    ref = oracle.reference_dir()
+    if ref is None:
+        raise SystemExit("set TILESTREAM_REFERENCE to the reference checkout")
+    return ref
+
+
+def copy_reference_inputs(ref: str) -> None:
+    """fuzz_corpus.npz (key '<corpus>/<file name>', the file's bytes) and datasets/*.npy."""
+    corpus = {}
+    for kind in ("parse", "mutation"):
+        folder = os.path.join(ref, "fuzz", "corpus", kind)
+        for name in sorted(os.listdir(folder)):
+            with open(os.path.join(folder, name), "rb") as f:
+                corpus[f"{kind}/{name}"] = np.frombuffer(f.read(), np.uint8)
+    np.savez_compressed(os.path.join(HERE, "fuzz_corpus.npz"), **corpus)
+    out = os.path.join(HERE, "datasets")
+    os.makedirs(out, exist_ok=True)
+    folder = os.path.join(ref, "datasets", "fixtures")
+    for name in sorted(os.listdir(folder)):
+        if name.endswith(".npy"):
+            shutil.copyfile(os.path.join(folder, name), os.path.join(out, name))
+
+
 def contract_rows():
     """The rows of the reference's contract_rows[] table, read from its header text."""
-    with open(os.path.join(oracle.REFERENCE_DIR, "tests", "numerics", "support.h")) as f:
+    with open(os.path.join(reference_checkout(), "tests", "numerics", "support.h")) as f:
         text = f.read()
     block = text[text.index("contract_rows[] = {"):]
     block = block[:block.index("};")]
@@ -85,6 +116,8 @@ def same_word(got: int, want: int) -> bool:
 
 
 def main():
+    ref_dir = reference_checkout()
+    copy_reference_inputs(ref_dir)
     rows = contract_rows()
     words = lambda key: np.array([[int(r[key], 16) for r in rows]], np.uint32)  # noqa: E731
     got = oracle.Oracle().calibrate_image(words("x"), words("offset").view(np.float32),
@@ -105,7 +138,7 @@ def main():
             f.write(to_hex(data))
         manifest[name] = {"width": w, "height": h, "type": ptype, "mode": mode,
                           "pixels": [int(v) for v in pixels]}
-        upstream = os.path.join(oracle.REFERENCE_DIR, "tests", "golden", name + ".hex")
+        upstream = os.path.join(ref_dir, "tests", "golden", name + ".hex")
         if os.path.exists(upstream):
             assert read_hex(upstream) == data, f"{name}: differs from the reference golden file"
     with open(os.path.join(HERE, "cases.json"), "w") as f:

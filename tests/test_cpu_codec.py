@@ -78,17 +78,13 @@ def test_field_frame_special_words(oracle_lib):
 
 
 def _dataset_fixtures():
-    path = os.path.join(oracle.REFERENCE_DIR, "datasets", "fixtures")
-    if not os.path.isdir(path):
-        pytest.skip("reference dataset fixtures not present")
-    for name in sorted(os.listdir(path)):
-        if name.endswith(".npy"):
-            yield name, np.load(os.path.join(path, name), allow_pickle=False)
+    from golden import inputs
+    yield from inputs.datasets()
 
 
 def test_dataset_fixtures_match_reference(oracle_lib, reference):
-    """The reference's committed image fixtures (datasets/fixtures/*.npy: a CT slice, an
-    elevation field and two generated images, read in place): for every tile shape the library's
+    """The reference's image fixtures (datasets/fixtures/*.npy: a CT slice, an elevation field
+    and two generated images, copied into tests/golden/datasets by make_golden.py): for every tile shape the library's
     encoder, the oracle and the reference build emit the same bytes, and the file decodes back
     to the same words."""
     seen = 0

@@ -168,12 +168,8 @@ def test_empty_and_null_sources():
 
 
 def _corpus(kind):
-    path = os.path.join(oracle.REFERENCE_DIR, "fuzz", "corpus", kind)
-    if not os.path.isdir(path):
-        pytest.skip("reference fuzz corpus not present")
-    for name in sorted(os.listdir(path)):
-        with open(os.path.join(path, name), "rb") as f:
-            yield name, f.read()
+    from golden import inputs
+    yield from inputs.corpus(kind)
 
 
 def test_parse_corpus_replay(oracle_lib, reference):

@@ -4,9 +4,8 @@ It serves callers that cannot allocate device memory while they encode (GPU memo
 full by another allocator, acquisition loops that must not stall on an allocator, deployments
 without dynamic allocation after start-up). Its scratch is a fixed array in device memory shared
 by every call, so these tests check that two calls in a row - the second reusing what the first
-left in the array - each produce exactly the file of the plan-based compress_async path, which
-is byte-identical to the CPU oracle in the other tests. The file is named so that pytest
-collects it last.
+left in the array - each produce exactly the file of the plan-based compress_async path and of
+the CPU oracle. The file is named so that pytest collects it last.
 """
 import ctypes as C
 
@@ -56,7 +55,7 @@ def record(result):
     return int(r[0]), int(r[1]), int(r[2]) | (int(r[3]) << 32)
 
 
-def test_two_calls_in_a_row_match_the_plan_path(cuda_ready):
+def test_two_calls_in_a_row_match_the_plan_path(cuda_ready, oracle_lib):
     torch = cuda_ready
     stream = torch.cuda.current_stream()
     first = workloads.detector_frame(1000, 700, seed=61)        # 8 x 22 tiles of 128x32
@@ -74,6 +73,7 @@ def test_two_calls_in_a_row_match_the_plan_path(cuda_ready):
         assert got_rec == want_rec
         data = host(out)
         assert data[:got_rec[2]].tobytes() == want
+        assert want == oracle_lib.compress_image(frame, tile)
         assert np.all(data[bound:] == SENTINEL)
     # Again in the other order: the array now holds the larger image's flags.
     for frame, ptype, tile in reversed(calls):

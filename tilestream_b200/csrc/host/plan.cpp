@@ -29,33 +29,43 @@ namespace detail {
 
 constexpr std::uint32_t kWindowTiles = 4096; // the reference's window bound (plan.h:14)
 
+// One sweep over every non-empty range in order of its first byte. A range overlaps an earlier
+// one exactly when it starts before that one ends, so it is enough to carry two high-water
+// marks: the furthest end of any earlier range and of any earlier writable range. The same
+// sweep builds the coalesced union that disjoint() searches.
 bool RangeSet::assign(std::vector<Range> writable, std::vector<Range> readable) {
-    auto empty = [](const Range &r) { return r.begin == r.end; };
-    auto by_begin = [](const Range &a, const Range &b) { return a.begin < b.begin; };
-    writable.erase(std::remove_if(writable.begin(), writable.end(), empty), writable.end());
-    readable.erase(std::remove_if(readable.begin(), readable.end(), empty), readable.end());
-    std::sort(writable.begin(), writable.end(), by_begin);
-    std::sort(readable.begin(), readable.end(), by_begin);
-    for (std::size_t i = 1; i < writable.size(); ++i) {
-        if (writable[i].begin < writable[i - 1].end) {
-            return false;
-        }
-    }
-    std::vector<std::uintptr_t> max_end(readable.size());
-    std::uintptr_t reach = 0;
-    for (std::size_t i = 0; i < readable.size(); ++i) {
-        reach = std::max(reach, readable[i].end);
-        max_end[i] = reach;
-    }
-    readable_ = std::move(readable);
-    max_end_ = std::move(max_end);
-    writable_.clear();
+    struct Tagged {
+        Range range;
+        bool writes;
+    };
+    std::vector<Tagged> all;
+    all.reserve(writable.size() + readable.size());
     for (const Range &r : writable) {
-        if (!disjoint(r)) {
+        if (r.end != r.begin) all.push_back({r, true});
+    }
+    for (const Range &r : readable) {
+        if (r.end != r.begin) all.push_back({r, false});
+    }
+    std::sort(all.begin(), all.end(),
+              [](const Tagged &a, const Tagged &b) { return a.range.begin < b.range.begin; });
+    std::uintptr_t any_end = 0, written_end = 0;
+    std::vector<Range> spans;
+    for (const Tagged &t : all) {
+        const bool clash = t.writes ? t.range.begin < any_end : t.range.begin < written_end;
+        if (clash) {
             return false;
         }
+        if (!spans.empty() && t.range.begin <= spans.back().end) {
+            spans.back().end = std::max(spans.back().end, t.range.end);
+        } else {
+            spans.push_back(t.range);
+        }
+        any_end = std::max(any_end, t.range.end);
+        if (t.writes) {
+            written_end = std::max(written_end, t.range.end);
+        }
     }
-    writable_ = std::move(writable);
+    spans_ = std::move(spans);
     return true;
 }
 
@@ -63,16 +73,10 @@ bool RangeSet::disjoint(Range range) const noexcept {
     if (range.begin == range.end) {
         return true;
     }
-    auto starts_before = [](const Range &r, std::uintptr_t end) { return r.begin < end; };
-    // Writable ranges are disjoint and sorted: only the last one starting before range.end can
-    // reach into it.
-    auto w = std::lower_bound(writable_.begin(), writable_.end(), range.end, starts_before);
-    if (w != writable_.begin() && std::prev(w)->end > range.begin) {
-        return false;
-    }
-    auto r = std::lower_bound(readable_.begin(), readable_.end(), range.end, starts_before);
-    const auto n = static_cast<std::size_t>(r - readable_.begin());
-    return n == 0 || max_end_[n - 1] <= range.begin;
+    // The first span that ends after range.begin is the only candidate for an overlap.
+    const auto it = std::upper_bound(spans_.begin(), spans_.end(), range.begin,
+                                     [](std::uintptr_t at, const Range &s) { return at < s.end; });
+    return it == spans_.end() || it->begin >= range.end;
 }
 
 PlanState::~PlanState() {

@@ -16,17 +16,19 @@ struct Range {
     std::uintptr_t end = 0;
 };
 
-// Writable ranges are pairwise disjoint and disjoint from every readable range; readable
-// ranges may overlap one another (docs/api.md:146-148).
+// The byte ranges one plan touches. Writable ranges may overlap nothing else; readable ranges
+// may overlap one another (docs/api.md "Aliasing"). After a successful assign() the set keeps
+// only the union of all its ranges, coalesced into sorted disjoint spans, which is what an
+// execution's workspace and result records are checked against.
 class RangeSet {
   public:
+    // False when a writable range overlaps any other range of either kind.
     [[nodiscard]] bool assign(std::vector<Range> writable, std::vector<Range> readable);
+    // True when `range` shares no byte with any range of the set (empty ranges share none).
     [[nodiscard]] bool disjoint(Range range) const noexcept;
 
   private:
-    std::vector<Range> writable_;
-    std::vector<Range> readable_;
-    std::vector<std::uintptr_t> max_end_; // max end of readable_[0..i]
+    std::vector<Range> spans_; // sorted by begin, pairwise disjoint and non-adjacent
 };
 
 inline Range range_of(const void *data, std::uint64_t size) noexcept {

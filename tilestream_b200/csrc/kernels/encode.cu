@@ -945,42 +945,57 @@ __global__ void __launch_bounds__(kThreads, AnyF32 ? 3 : 4)
     encode_chunks<AnyF32>(sh, SingleImage{&image}, total_tiles, chunk_tiles, state, result);
 }
 
-// Per-device set-up, done by the first call on each device with that device current.
+// Per-device set-up, done by the first call on each device with that device current: the
+// persistent grids of the two instances, from their occupancy. The scratch address and the
+// shared-memory attribute are not cached (see static_launch_state), so a device reset between
+// calls, which may place the module elsewhere, leaves nothing stale.
 struct StaticSetup {
-    uint64_t *scratch = nullptr; // device address of g_encode_scratch
-    uint32_t grid[2] = {0, 0};   // persistent grids of the uint16 and FP32 instances
+    uint32_t grid[2] = {0, 0}; // persistent grids of the uint16 and FP32 instances
 };
 
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mutex;
 StaticSetup g_setup[kMaxDevices];
 
+template <bool F32> cudaError_t set_static_smem() {
+    return cudaFuncSetAttribute(encode_kernel_static<F32>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(sizeof(SharedFor<F32>)));
+}
+
 cudaError_t static_setup(int device, StaticSetup &out) {
     std::lock_guard<std::mutex> lock(g_setup_mutex);
     StaticSetup &s = g_setup[device];
-    if (s.scratch == nullptr) {
-        void *address = nullptr;
-        // In host code the name g_encode_scratch is a host-side stand-in, not a device address;
-        // the runtime returns this device's copy of the array.
-        cudaError_t e = cudaGetSymbolAddress(&address, g_encode_scratch);
-        if (e != cudaSuccess) return e;
+    if (s.grid[0] == 0) {
         int sms = 0;
-        e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
         if (e != cudaSuccess) return e;
         for (int f32 = 0; f32 < 2; ++f32) {
             auto kernel = f32 ? encode_kernel_static<true> : encode_kernel_static<false>;
             const size_t smem = f32 ? sizeof(SharedFor<true>) : sizeof(SharedFor<false>);
-            e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     static_cast<int>(smem));
+            e = f32 ? set_static_smem<true>() : set_static_smem<false>();
             if (e != cudaSuccess) return e;
             int per_sm = 0;
             e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, smem);
             if (e != cudaSuccess) return e;
             s.grid[f32] = static_cast<uint32_t>(sms * (per_sm > 0 ? per_sm : 1));
         }
-        s.scratch = static_cast<uint64_t *>(address);
     }
     out = s;
+    return cudaSuccess;
+}
+
+// What every call looks up afresh (cheap host queries that allocate nothing): the current
+// device's address of g_encode_scratch, and the instance's shared-memory limit. In host code
+// the name g_encode_scratch is a host-side stand-in, not a device address; the runtime
+// returns this device's copy of the array.
+cudaError_t static_launch_state(bool f32, uint64_t *&scratch) {
+    void *address = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&address, g_encode_scratch);
+    if (e != cudaSuccess) return e;
+    e = f32 ? set_static_smem<true>() : set_static_smem<false>();
+    if (e != cudaSuccess) return e;
+    scratch = static_cast<uint64_t *>(address);
     return cudaSuccess;
 }
 
@@ -1005,6 +1020,9 @@ extern "C" int tsk_encode_static_launch(const tsk_encode_image *image, tsk_resul
     e = tsk::static_setup(device, setup);
     if (e != cudaSuccess) return e;
     const bool f32 = image->type == 2;
+    uint64_t *scratch = nullptr;
+    e = tsk::static_launch_state(f32, scratch);
+    if (e != cudaSuccess) return e;
     const uint32_t full = setup.grid[f32 ? 1 : 0];
     const uint32_t k = tsk::chunk_tiles_for(total, full, f32);
     const uint64_t chunks = (total + k - 1) / k;
@@ -1012,13 +1030,13 @@ extern "C" int tsk_encode_static_launch(const tsk_encode_image *image, tsk_resul
     const uint64_t words = tsk::state_words(chunks);
     if (words > tsk::kStaticStateWords) return cudaErrorInvalidValue;
     // The array keeps the previous call's contents: clear the counter and this call's words.
-    e = cudaMemsetAsync(setup.scratch, 0, 8 * words, stream);
+    e = cudaMemsetAsync(scratch, 0, 8 * words, stream);
     if (e != cudaSuccess) return e;
     e = cudaMemsetAsync(result, 0, sizeof(tsk_result), stream);
     if (e != cudaSuccess) return e;
     auto kernel = f32 ? tsk::encode_kernel_static<true> : tsk::encode_kernel_static<false>;
     const size_t smem = f32 ? sizeof(tsk::SharedFor<true>) : sizeof(tsk::SharedFor<false>);
     kernel<<<static_cast<uint32_t>(grid), tsk::kThreads, smem, stream>>>(*image, total, k,
-                                                                         setup.scratch, result);
+                                                                         scratch, result);
     return cudaGetLastError();
 }
