@@ -232,6 +232,33 @@ int ts_compress_noalloc(ts_const_image_view input, ts_tile_shape tile, ts_mutabl
                         ts_device_result *result, void *stream);
 uint64_t ts_compress_noalloc_max_tiles(void);
 
+/* ---- plan inspection (extension, no reference counterpart) ---------------------------------
+ * For validation tooling. Runs the host half of ts_prepare_batch for a decode request
+ * (decompress, decode_roi or decode_calibrate): every argument, metadata, ROI, capacity and
+ * aliasing check that needs no device, then the planning of its tile tasks. It never touches
+ * a device and dereferences no buffer pointer, so any address values may stand in for device
+ * buffers. Returns the status of those checks (device and pointer checks are not made).
+ * *count receives the number of tasks; the first min(*count, capacity) are described:
+ *   read_begin/read_end    the bytes the task stages (a parsed tile's payload; for an
+ *                          encoder-output source, the whole archive buffer, whose index entry
+ *                          and row descriptors the kernel validates itself)
+ *   write_begin/write_end  the first and one past the last output byte it may write
+ *   rows_end               parsed predictive tiles: one past the furthest row descriptor,
+ *                          relative to read_begin (0 otherwise)
+ *   mode, flags            the tile mode (0 raw, 1 constant, 2 predict) and task flags
+ *                          (1 FP32, 2 calibrated, 4 encoder output, 8 first of its image,
+ *                          16 whole aligned rows) */
+typedef struct {
+    uint64_t image;
+    uint64_t read_begin, read_end;
+    uint64_t write_begin, write_end;
+    uint64_t rows_end;
+    uint32_t mode, flags;
+    uint32_t width, height;
+} ts_task_span;
+int ts_inspect_decode(const ts_batch_request *request, ts_task_span *spans, uint64_t capacity,
+                      uint64_t *count);
+
 /* ---- device buffers and completion (cuda.h:113-145) ----------------------------------------
  * Stream-ordered allocation aligned to 256 bytes; *data is replaced only on success. */
 int ts_device_allocate(uint64_t bytes, void *stream, void **data);

@@ -98,6 +98,12 @@ class Oracle:
         lib.tso_case.argtypes = [u64, C.POINTER(u32), C.POINTER(u64), vp]
         lib.tso_fill.argtypes = [u32, u32, u32, u64, u32, u64, vp]
         lib.tso_mutation_build.argtypes = [vp, u64, vp, u64, C.POINTER(u64)]
+        lib.tso_rng_new.argtypes = [u64]
+        lib.tso_rng_new.restype = vp
+        lib.tso_rng_free.argtypes = [vp]
+        lib.tso_rng_next.argtypes = [vp]
+        lib.tso_rng_next.restype = u64
+        lib.tso_fabricate.argtypes = [vp, vp, C.POINTER(u64), vp, C.POINTER(u64), C.POINTER(u64)]
         self.lib = lib
 
     # --- sizes -----------------------------------------------------------------------------
@@ -211,6 +217,23 @@ class Oracle:
         self.lib.tso_fill(ptype, width, height, pitch, pattern, seed, _ptr(buf))
         return buf
 
+    def engine(self, seed: int) -> "Engine":
+        """A std::mt19937_64 engine shared by Python draws and fabricate()."""
+        return Engine(self.lib, seed)
+
+    def fabricate(self, engine: "Engine", tiles: np.ndarray, segments: np.ndarray,
+                  file_bytes: int):
+        """One fabricated change of parsed metadata (tests/cuda_robustness_test.cpp:194-243):
+        returns (tiles, segments, file_bytes) copies with one field changed or one record
+        dropped. tiles/segments use TILE_DTYPE/SEGMENT_DTYPE."""
+        t = np.ascontiguousarray(tiles.copy())
+        g = np.zeros(len(segments) + 1, SEGMENT_DTYPE)
+        g[:len(segments)] = segments
+        nt, ng, fb = C.c_uint64(len(t)), C.c_uint64(len(segments)), C.c_uint64(file_bytes)
+        self.lib.tso_fabricate(engine.handle, _ptr(t), C.byref(nt), _ptr(g), C.byref(ng),
+                               C.byref(fb))
+        return t[:nt.value].copy(), g[:ng.value].copy(), fb.value
+
     def mutation_file(self, corpus_input: bytes):
         """Rebuilds the mutated .tsc file of one reference mutation-corpus input, or None."""
         cap = 1 << 22
@@ -220,6 +243,22 @@ class Oracle:
         rc = self.lib.tso_mutation_build(_ptr(src), len(corpus_input), _ptr(out), cap,
                                          C.byref(size))
         return None if rc else out[:size.value].tobytes()
+
+
+class Engine:
+    """std::mt19937_64 in the oracle library; next() is one engine draw."""
+
+    def __init__(self, lib, seed: int):
+        self.lib = lib
+        self.handle = lib.tso_rng_new(seed)
+
+    def next(self) -> int:
+        return int(self.lib.tso_rng_next(self.handle))
+
+    def __del__(self):
+        if getattr(self, "handle", None):
+            self.lib.tso_rng_free(self.handle)
+            self.handle = None
 
 
 class Reference:

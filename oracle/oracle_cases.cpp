@@ -200,6 +200,81 @@ void tso_fill(std::uint32_t type, std::uint32_t width, std::uint32_t height, std
     fill(type, width, height, pitch, pattern, seed, bytes);
 }
 
+// ---- fabricated metadata (tests/cuda_robustness_test.cpp:194-243) -------------------------
+// One std::mt19937_64 engine that the Python side draws from between fabrications (the ROI of
+// each trial), so the whole campaign consumes the engine in the reference test's order.
+void *tso_rng_new(std::uint64_t seed) {
+    return new std::mt19937_64(seed);
+}
+void tso_rng_free(void *rng) {
+    delete static_cast<std::mt19937_64 *>(rng);
+}
+std::uint64_t tso_rng_next(void *rng) {
+    return (*static_cast<std::mt19937_64 *>(rng))();
+}
+
+// Host metadata records with the layout of the library's TileMetadata (32 bytes) and
+// SegmentMetadata (24 bytes).
+struct FabTile {
+    std::uint32_t mode;
+    std::uint16_t width, height;
+    std::uint64_t offset, length, first_segment;
+};
+struct FabSegment {
+    std::uint32_t seed, bit_width;
+    std::uint64_t payload_offset, payload_bytes;
+};
+
+// A field moved by a small multiple of `step`, or (one time in three) replaced by an arbitrary
+// value: 64 random bits one time in three of those, else a value below 65536. Arithmetic is
+// modulo 2^64, as in the reference.
+static std::uint64_t nudge(std::uint64_t value, std::mt19937_64 &rng, std::uint64_t step) {
+    if (rng() % 3 == 0) {
+        if (rng() % 3 == 0) return rng();
+        return rng() % 65536;
+    }
+    const std::uint64_t k = rng() % 17;
+    return value + (k - 8) * step;
+}
+
+// Changes one field of the metadata, drawing in the reference's order: the tile, then the
+// segment (a default segment is appended when there is none), then the field among twelve.
+// The last case drops the final tile or (when there are segments) the final segment.
+// *tile_count and *segment_count are updated; the arrays must hold one spare segment.
+void tso_fabricate(void *engine, FabTile *tiles, std::uint64_t *tile_count,
+                   FabSegment *segments, std::uint64_t *segment_count, std::uint64_t *file_bytes) {
+    auto &rng = *static_cast<std::mt19937_64 *>(engine);
+    FabTile &tile = tiles[rng() % *tile_count];
+    FabSegment *segment = nullptr;
+    if (*segment_count == 0) {
+        segments[0] = FabSegment{};
+        *segment_count = 1;
+        segment = &segments[0];
+    } else {
+        segment = &segments[rng() % *segment_count];
+    }
+    switch (rng() % 12) {
+    case 0: tile.mode = static_cast<std::uint32_t>(rng() % 4); break;
+    case 1: tile.width = static_cast<std::uint16_t>(nudge(tile.width, rng, 1)); break;
+    case 2: tile.height = static_cast<std::uint16_t>(nudge(tile.height, rng, 1)); break;
+    case 3: tile.offset = nudge(tile.offset, rng, 4); break;
+    case 4: tile.length = nudge(tile.length, rng, 4); break;
+    case 5: tile.first_segment = nudge(tile.first_segment, rng, 1); break;
+    case 6: segment->seed = static_cast<std::uint32_t>(nudge(segment->seed, rng, 1)); break;
+    case 7: segment->bit_width = static_cast<std::uint32_t>(rng() % 40); break;
+    case 8: segment->payload_offset = nudge(segment->payload_offset, rng, 4); break;
+    case 9: segment->payload_bytes = nudge(segment->payload_bytes, rng, 4); break;
+    case 10: *file_bytes = nudge(*file_bytes, rng, 4); break;
+    default:
+        if (rng() % 2 == 0) {
+            --*tile_count;
+        } else if (*segment_count != 0) {
+            --*segment_count;
+        }
+        break;
+    }
+}
+
 // harness.h:227-290: rebuilds the mutated .tsc file described by one mutation-corpus input.
 // Returns 0 and the file in out (capacity cap) or a nonzero code when the corpus input does not
 // describe a valid starting image or the file does not fit.

@@ -109,6 +109,12 @@ class ResultBuffer(C.Structure):
     _fields_ = [("data", vp), ("count", u64)]
 
 
+class TaskSpan(C.Structure):
+    _fields_ = [("image", u64), ("read_begin", u64), ("read_end", u64), ("write_begin", u64),
+                ("write_end", u64), ("rows_end", u64), ("mode", u32), ("flags", u32),
+                ("width", u32), ("height", u32)]
+
+
 class MixedItem(C.Structure):
     _fields_ = [("operation", u32), ("item", BatchItem)]
 
@@ -166,6 +172,8 @@ _SIGNATURES = {
     "ts_cpu_decompress": (C.c_int, [ConstBytes, ImageView, C.POINTER(ParseLimits)]),
     "ts_prepare_batch": (C.c_int, [C.POINTER(BatchRequest), C.POINTER(vp), vp]),
     "ts_plan_destroy": (None, [vp]),
+    "ts_inspect_decode": (C.c_int, [C.POINTER(BatchRequest), C.POINTER(TaskSpan), u64,
+                                    C.POINTER(u64)]),
     "ts_plan_workspace_spec": (C.c_int, [vp, C.POINTER(WorkspaceSpec)]),
     "ts_compress_async": (C.c_int, [vp, MutableBytes, ResultBuffer, vp]),
     "ts_decompress_async": (C.c_int, [vp, MutableBytes, ResultBuffer, vp]),

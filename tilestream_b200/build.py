@@ -2,7 +2,8 @@
 
 `build()` is incremental: a stamp holds the SHA-256 of every source, header and flag, and the
 library is rebuilt only when that changes. The result is tilestream_b200/libtilestream_b200.so,
-which the Python package loads with ctypes; nothing is installed outside the repository.
+which the Python package loads with ctypes, and libtilestream_b200.a (the same objects) for
+C++ programs that link the library statically; nothing is installed outside the repository.
 """
 from __future__ import annotations
 
@@ -19,6 +20,9 @@ CSRC = os.path.join(PKG, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 BUILD = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "libtilestream_b200.so")
+# The same objects as a static archive, for C++ programs that link the library into one
+# executable with one CUDA runtime (the reference's test suites, tests/reference_suite).
+ARCHIVE = os.path.join(PKG, "libtilestream_b200.a")
 
 CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
@@ -55,7 +59,7 @@ def fingerprint() -> str:
 
 def up_to_date() -> bool:
     stamp = os.path.join(BUILD, "stamp")
-    if not os.path.exists(LIB) or not os.path.exists(stamp):
+    if not os.path.exists(LIB) or not os.path.exists(ARCHIVE) or not os.path.exists(stamp):
         return False
     with open(stamp) as f:
         return f.read().strip() == fingerprint()
@@ -89,6 +93,11 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if r.returncode != 0:
         raise RuntimeError(f"link failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
     os.replace(tmp, LIB)
+    if os.path.exists(ARCHIVE):
+        os.remove(ARCHIVE)
+    r = subprocess.run(["ar", "rcs", ARCHIVE] + objs, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"archive failed: {r.stdout}\n{r.stderr}")
     with open(os.path.join(BUILD, "stamp"), "w") as f:
         f.write(fingerprint())
     if verbose:

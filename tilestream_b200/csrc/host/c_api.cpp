@@ -55,6 +55,7 @@ static_assert(std::is_trivially_copyable_v<ts::cuda::DeviceImage> &&
               std::is_standard_layout_v<ts::cuda::DeviceBatch>);
 
 TS_SAME_LAYOUT(ts_mixed_item, ts::cuda::MixedItem);
+TS_SAME_LAYOUT(ts_task_span, ts::cuda::detail::TaskSpan);
 TS_SAME_LAYOUT(ts_mixed_stats, ts::cuda::MixedStats);
 static_assert(offsetof(ts_mixed_item, item) == offsetof(ts::cuda::MixedItem, item));
 
@@ -219,6 +220,35 @@ int ts_prepare_batch(const ts_batch_request *request, ts_plan **plan, void *stre
         if (st == ts::Status::success) {
             delete *plan;
             *plan = holder.release();
+        }
+        return code(st);
+    } catch (...) {
+        return code(ts::Status::resource_limit);
+    }
+}
+
+int ts_inspect_decode(const ts_batch_request *request, ts_task_span *spans, uint64_t capacity,
+                      uint64_t *count) {
+    if (request == nullptr || count == nullptr || (capacity != 0 && spans == nullptr)) {
+        return code(ts::Status::invalid_argument);
+    }
+    try {
+        ts::cuda::BatchRequest r = as<ts::cuda::BatchRequest>(*request);
+        std::vector<ts::cuda::BatchItem> items;
+        if (request->items != nullptr && request->count <= UINT32_MAX) {
+            items.resize(request->count);
+            for (uint64_t i = 0; i < request->count; ++i) {
+                items[i] = as<ts::cuda::BatchItem>(request->items[i]);
+                const ts_metadata *m = request->items[i].compressed_input.metadata;
+                items[i].compressed_input.metadata = m != nullptr ? &m->value : nullptr;
+            }
+            r.items = items.data();
+        }
+        std::vector<ts::cuda::detail::TaskSpan> found;
+        const ts::Status st = ts::cuda::detail::inspect_decode(r, found);
+        *count = found.size();
+        for (uint64_t i = 0; i < found.size() && i < capacity; ++i) {
+            spans[i] = as<ts_task_span>(found[i]);
         }
         return code(st);
     } catch (...) {

@@ -866,6 +866,69 @@ WorkspaceSpec BatchPlan::workspace_spec() const noexcept {
     return impl_ != nullptr ? impl_->spec : WorkspaceSpec{};
 }
 
+namespace detail {
+
+// The host half of prepare_batch for a decode request (drafting and the aliasing rule; no
+// device, pointer or allocation step), reported task by task.
+Status inspect_decode(const BatchRequest &request, std::vector<TaskSpan> &spans) {
+    spans.clear();
+    if (request.count > UINT32_MAX) {
+        return Status::resource_limit;
+    }
+    if (request.count != 0 && request.items == nullptr) {
+        return Status::invalid_argument;
+    }
+    if (request.operation != Operation::decompress && request.operation != Operation::decode_roi &&
+        request.operation != Operation::decode_calibrate) {
+        return Status::invalid_argument;
+    }
+    if (request.count == 0) {
+        return Status::success;
+    }
+    Draft d;
+    Status st = draft_decode(request, d);
+    if (st != Status::success) {
+        return st;
+    }
+    RangeSet ranges;
+    if (!ranges.assign(d.writable, d.readable)) {
+        return Status::invalid_argument;
+    }
+    spans.reserve(d.tasks.size());
+    for (const tsk_decode_task &t : d.tasks) {
+        const tsk_decode_image &im = d.images[t.image];
+        TaskSpan s;
+        s.image = t.image;
+        s.mode = t.mode;
+        s.flags = t.flags;
+        s.width = t.width;
+        s.height = t.height;
+        if (t.flags & TSK_TRUSTED) {
+            s.read_begin = t.src;
+            s.read_end = t.src + im.capacity;
+        } else {
+            s.read_begin = t.src;
+            s.read_end = t.src + 4 * t.words_or_tile;
+            if (t.mode == TSK_PREDICT) {
+                for (std::uint32_t r = 0; r < t.height; ++r) {
+                    s.rows_end = std::max<std::uint64_t>(
+                        s.rows_end, 4ull * d.rows[t.rows_at + r] + format::segment_header_bytes);
+                }
+            }
+        }
+        const std::uint64_t esize = (t.flags & (TSK_F32 | TSK_CALIBRATED)) ? 4 : 2;
+        if (t.row1 > t.row0 && t.col1 > t.col0) {
+            s.write_begin = t.dst + std::uint64_t{t.col0} * esize;
+            s.write_end = t.dst + std::uint64_t(t.row1 - t.row0 - 1) * t.pitch +
+                          std::uint64_t{t.col1} * esize;
+        }
+        spans.push_back(s);
+    }
+    return Status::success;
+}
+
+} // namespace detail
+
 Status prepare_batch(const BatchRequest &request, std::unique_ptr<BatchPlan> &plan,
                      cudaStream_t stream) noexcept {
     if (request.count > UINT32_MAX) {

@@ -96,6 +96,20 @@ struct PlanState {
 // The structural checks of tile `index` that keep device reads inside its payload.
 [[nodiscard]] Status check_tile(const ImageMetadata &m, std::uint64_t index) noexcept;
 
+// One tile task of a decode plan as the host planned it (inspect_decode): the bytes it stages,
+// the output bytes it may write, and for parsed predictive tiles the end of its furthest row
+// descriptor relative to read_begin.
+struct TaskSpan {
+    std::uint64_t image = 0;
+    std::uint64_t read_begin = 0, read_end = 0;
+    std::uint64_t write_begin = 0, write_end = 0;
+    std::uint64_t rows_end = 0;
+    std::uint32_t mode = 0, flags = 0;
+    std::uint32_t width = 0, height = 0;
+};
+
+[[nodiscard]] Status inspect_decode(const BatchRequest &request, std::vector<TaskSpan> &spans);
+
 [[nodiscard]] Status check_execution(const PlanState *plan, Operation operation,
                                      MutableBytes workspace, ResultBuffer results,
                                      cudaStream_t stream) noexcept;

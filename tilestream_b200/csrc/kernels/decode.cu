@@ -60,9 +60,18 @@ struct StageHeader {
 
 // MaxPayload: the largest tile payload of the plan (8 KiB for uint16-only plans, 16 KiB with
 // FP32). Each stage adds alignment shift and over-read slack.
+//
+// Reads stay inside the shared allocation for any payload bytes. A row's residual width comes
+// from its descriptor in the payload, clamped to 16 (uint16) or 32 (FP32) bits, and the planner
+// keeps every row start inside the payload (check_tile), so a lane's windows end at most
+// 8 + 4 * ((width + 28) * bits / 32 + 3) bytes past a row start: 1044 bytes for a 256-wide FP32
+// row, 584 for uint16. Metadata built by hand can point a row start anywhere in the payload;
+// then the reads of one stage may run into the next stage, and those of the last stage (payload
+// end + alignment shift + that reach, less the stage's 128 bytes of slack) into `tail`.
 template <uint32_t MaxPayload, uint32_t Stages> struct Shared {
     static constexpr uint32_t kStage = MaxPayload + 128;
     alignas(128) uint8_t payload[Stages][kStage];
+    uint8_t tail[MaxPayload > 8192 ? 1152 : 640];
     alignas(16) uint16_t rows[Stages][TSK_MAX_ROWS];
     alignas(16) StageHeader header[Stages];
     alignas(8) uint64_t full[Stages];
@@ -386,7 +395,8 @@ __device__ void decode_rows(const Ctx &x, const uint32_t *payload, const uint16_
         }
         if (mode == TSK_PREDICT) {
             const uint32_t *row = payload + (live ? rows[r] : 0u);
-            const uint32_t b = live ? (row[1] & 0xffu) : 0u;
+            const uint32_t width_byte = live ? (row[1] & 0xffu) : 0u;
+            const uint32_t b = width_byte < (F32 ? 32u : 16u) ? width_byte : (F32 ? 32u : 16u);
             const uint32_t *packed = row + 2;
             // The seed is the initial carry: value(c) = seed (+ or ^) the terms of items 0..c.
             uint32_t carry = live ? row[0] : 0u;

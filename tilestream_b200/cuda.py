@@ -75,6 +75,16 @@ def prepare_batch(request: BatchRequest, plan: BatchPlan | None = None, stream=N
     return Status(st), plan
 
 
+def inspect_decode(request: BatchRequest):
+    """Host-only planning of a decode request (ts_inspect_decode): (Status, [TaskSpan...]).
+    No device is touched, so the request may carry stand-in addresses."""
+    count = C.c_uint64(0)
+    st = N.lib().ts_inspect_decode(C.byref(request), None, 0, C.byref(count))
+    spans = (N.TaskSpan * max(1, count.value))()
+    st = N.lib().ts_inspect_decode(C.byref(request), spans, count.value, C.byref(count))
+    return Status(st), list(spans[:count.value])
+
+
 def _results(results) -> ResultBuffer:
     if isinstance(results, ResultBuffer):
         return results
