@@ -53,7 +53,9 @@ def fingerprint() -> str:
         h.update(os.path.relpath(path, ROOT).encode())
         with open(path, "rb") as f:
             h.update(f.read())
-    h.update(" ".join(NVCC_FLAGS + CXX_FLAGS + LINK_FLAGS).encode())
+    # Flags name absolute include paths; hash them relative to the repository root so that a
+    # copy of the tree elsewhere (with its built library) is still up to date.
+    h.update(" ".join(NVCC_FLAGS + CXX_FLAGS + LINK_FLAGS).replace(ROOT, "<root>").encode())
     return h.hexdigest()
 
 
