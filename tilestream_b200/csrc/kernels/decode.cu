@@ -465,9 +465,130 @@ __device__ void decode_rows(const Ctx &x, const uint32_t *payload, const uint16_
     }
 }
 
-template <uint32_t CW, uint32_t G, uint32_t LW, bool F32, bool Cal>
+// Predictive uint16 rows. The class width G * LW covers every uint16 row (64, 128 or 256), so
+// a row is one pass of its LW lanes: no pass loop and no carry between passes. Each lane
+// decodes NR rows at once (rows r, r + R, ... with R = CW * 32 / LW), their steps interleaved so
+// that one row's shuffle scan and window loads overlap the other rows' arithmetic.
+template <uint32_t CW, uint32_t G, uint32_t LW, bool Cal, bool Full, uint32_t NR>
+__device__ __forceinline__ void predict_rows_u16(const Ctx &x, const uint32_t *payload,
+                                                 const uint16_t *rows) {
+    constexpr uint32_t kRowsPerWarp = 32 / LW;
+    constexpr uint32_t kStride = CW * kRowsPerWarp;
+    constexpr uint32_t H = G / 2;
+    const uint32_t warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const uint32_t sub = lane % LW;
+    const uint32_t c0 = sub * G;
+    const uint32_t w = x.w;
+    const Pipes pipes{x.one, x.top};
+    auto add = [&pipes](uint32_t a, uint32_t b) { return fma_add(a, b, pipes); };
+    auto prefetch_maps = [&](uint32_t row) {
+        if constexpr (Cal) {
+            if (row < x.row1 && c0 < x.col1 && c0 + G > x.col0) {
+                const uint64_t line = static_cast<uint64_t>(row - x.row0);
+                const uint32_t c = c0 > x.col0 ? c0 : x.col0;
+                const uint32_t e = (c0 + G < x.col1 ? c0 + G : x.col1) - 1;
+                if (x.omap) {
+                    const uint8_t *m = x.omap + line * x.opitch;
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(m + 4 * c));
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(m + 4 * e));
+                }
+                if (x.gmap) {
+                    const uint8_t *m = x.gmap + line * x.gpitch;
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(m + 4 * c));
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(m + 4 * e));
+                }
+            }
+        }
+    };
+    const uint32_t mine = x.row0 + warp * kRowsPerWarp + lane / LW;
+    if constexpr (Cal) {
+#pragma unroll
+        for (uint32_t n = 0; n < NR; ++n) {
+            prefetch_maps(mine + n * kStride);
+        }
+    }
+    for (uint32_t base = x.row0 + warp * kRowsPerWarp; base < x.row1; base += NR * kStride) {
+        uint32_t t[NR][G];
+        uint32_t carry[NR], total[NR], inclusive[NR];
+        bool live[NR];
+        uint64_t line_off[NR];
+#pragma unroll
+        for (uint32_t n = 0; n < NR; ++n) {
+            const uint32_t r = base + n * kStride + lane / LW;
+            live[n] = r < x.row1;
+            if constexpr (Cal) {
+                prefetch_maps(r + NR * kStride);
+            }
+            line_off[n] = static_cast<uint64_t>(live[n] ? r - x.row0 : 0u);
+            const uint32_t *row = payload + (live[n] ? rows[r] : 0u);
+            const uint32_t width_byte = row[1] & 0xffu;
+            const uint32_t b = width_byte < 16u ? width_byte : 16u;
+            carry[n] = row[0];
+            if (Full || c0 < w) {
+                terms<G, false, !Full>(row + 2, c0, w, b, pipes, t[n]);
+            } else {
+#pragma unroll
+                for (uint32_t k = 0; k < G; ++k) {
+                    t[n][k] = 0;
+                }
+            }
+        }
+#pragma unroll
+        for (uint32_t n = 0; n < NR; ++n) {
+#pragma unroll
+            for (uint32_t k = 1; k < G; ++k) {
+                if (k != H) {
+                    t[n][k] = add(t[n][k - 1], t[n][k]);
+                }
+            }
+            total[n] = add(t[n][H - 1], t[n][G - 1]);
+            inclusive[n] = total[n];
+        }
+#pragma unroll
+        for (uint32_t d = 1; d < LW; d <<= 1) {
+#pragma unroll
+            for (uint32_t n = 0; n < NR; ++n) {
+                const uint32_t other = __shfl_up_sync(kFull, inclusive[n], d, LW);
+                if (sub >= d) {
+                    inclusive[n] = add(other, inclusive[n]);
+                }
+            }
+        }
+#pragma unroll
+        for (uint32_t n = 0; n < NR; ++n) {
+            if (live[n]) {
+                const uint32_t before = add(carry[n], inclusive[n] - total[n]);
+                const uint32_t mid = add(before, t[n][H - 1]);
+                uint32_t v[G];
+#pragma unroll
+                for (uint32_t k = 0; k < G; ++k) {
+                    v[k] = add(k < H ? before : mid, t[n][k]);
+                }
+                uint8_t *line = x.out + line_off[n] * x.pitch;
+                const uint8_t *orow = nullptr, *grow = nullptr;
+                if constexpr (Cal) {
+                    orow = x.omap ? x.omap + line_off[n] * x.opitch : nullptr;
+                    grow = x.gmap ? x.gmap + line_off[n] * x.gpitch : nullptr;
+                }
+                store<G, false, Cal, Full>(x, line, orow, grow, c0, v);
+            }
+        }
+    }
+}
+
+template <uint32_t CW, uint32_t G, uint32_t LW, bool F32, bool Cal, uint32_t NR>
 __device__ __forceinline__ void decode_class(const Ctx &x, const uint32_t *payload,
                                              const uint16_t *rows, uint32_t mode) {
+    if constexpr (!F32 && NR != 0) {
+        if (mode == TSK_PREDICT) {
+            if (x.full) {
+                predict_rows_u16<CW, G, LW, Cal, true, NR>(x, payload, rows);
+            } else {
+                predict_rows_u16<CW, G, LW, Cal, false, NR>(x, payload, rows);
+            }
+            return;
+        }
+    }
     if (x.full) {
         decode_rows<CW, G, LW, F32, Cal, true>(x, payload, rows, mode);
     } else {
@@ -477,22 +598,24 @@ __device__ __forceinline__ void decode_class(const Ctx &x, const uint32_t *paylo
 
 // Width classes: a row of the class width is covered by LW = width / G lanes. uint16 rows take
 // G16 columns per lane (8 or 16), FP32 rows 4.
-template <uint32_t CW, uint32_t G16, bool F32, bool Cal>
+// NR: uint16 predictive rows decoded per lane at once by predict_rows_u16 (0 keeps them on
+// the generic decode_rows).
+template <uint32_t CW, uint32_t G16, bool F32, bool Cal, uint32_t NR>
 __device__ __forceinline__ void decode_tile(const Ctx &x, const uint32_t *payload,
                                             const uint16_t *rows, uint32_t mode) {
     if constexpr (!F32) {
         if (x.w > 128) {
-            decode_class<CW, G16, 256 / G16, false, Cal>(x, payload, rows, mode);
+            decode_class<CW, G16, 256 / G16, false, Cal, NR>(x, payload, rows, mode);
         } else if (x.w > 64) {
-            decode_class<CW, G16, 128 / G16, false, Cal>(x, payload, rows, mode);
+            decode_class<CW, G16, 128 / G16, false, Cal, NR>(x, payload, rows, mode);
         } else {
-            decode_class<CW, G16, 64 / G16, false, Cal>(x, payload, rows, mode);
+            decode_class<CW, G16, 64 / G16, false, Cal, NR>(x, payload, rows, mode);
         }
     } else {
         if (x.w > 64) {
-            decode_class<CW, 4, 32, true, Cal>(x, payload, rows, mode);
+            decode_class<CW, 4, 32, true, Cal, 0>(x, payload, rows, mode);
         } else {
-            decode_class<CW, 4, 16, true, Cal>(x, payload, rows, mode);
+            decode_class<CW, 4, 16, true, Cal, 0>(x, payload, rows, mode);
         }
     }
 }
@@ -730,7 +853,7 @@ __device__ void stage_task(Sh &sh, uint32_t s, const tsk_decode_task &t, const S
 // The persistent loop over a task source: CW consumer warps, G16 columns per lane for uint16
 // rows.
 template <uint32_t MaxPayload, uint32_t Stages, uint32_t Paths, uint32_t CW, uint32_t G16,
-          typename Source>
+          uint32_t NR, typename Source>
 __device__ __forceinline__ void decode_body(Source &source, const tsk_row_start *rowtab,
                                             tsk_result *results, uint32_t one, uint32_t top) {
     using Sh = Shared<MaxPayload, Stages>;
@@ -834,17 +957,17 @@ __device__ __forceinline__ void decode_body(Source &source, const tsk_row_start 
             const uint16_t *rows = sh.rows[s];
             if constexpr ((Paths & kU16) && (Paths & kPlain)) {
                 if (!f32 && !calibrated) {
-                    decode_tile<CW, G16, false, false>(x, payload, rows, hmode);
+                    decode_tile<CW, G16, false, false, NR>(x, payload, rows, hmode);
                 }
             }
             if constexpr ((Paths & kF32) && (Paths & kPlain)) {
-                if (f32 && !calibrated) decode_tile<CW, G16, true, false>(x, payload, rows, hmode);
+                if (f32 && !calibrated) decode_tile<CW, G16, true, false, NR>(x, payload, rows, hmode);
             }
             if constexpr ((Paths & kU16) && (Paths & kCal)) {
-                if (!f32 && calibrated) decode_tile<CW, G16, false, true>(x, payload, rows, hmode);
+                if (!f32 && calibrated) decode_tile<CW, G16, false, true, NR>(x, payload, rows, hmode);
             }
             if constexpr ((Paths & kF32) && (Paths & kCal)) {
-                if (f32 && calibrated) decode_tile<CW, G16, true, true>(x, payload, rows, hmode);
+                if (f32 && calibrated) decode_tile<CW, G16, true, true, NR>(x, payload, rows, hmode);
             }
         }
         __syncwarp();
@@ -890,14 +1013,14 @@ __device__ __forceinline__ void decode_body(Source &source, const tsk_row_start 
 
 // A planned queue (every plan and mixed batch); MinBlocks resident CTAs per SM.
 template <uint32_t MaxPayload, uint32_t Stages, uint32_t Paths, uint32_t CW, uint32_t G16,
-          uint32_t MinBlocks>
+          uint32_t MinBlocks, uint32_t NR>
 __global__ void __launch_bounds__(threads_of(CW), MinBlocks)
     decode_kernel(const tsk_decode_task *__restrict__ tasks, uint32_t ntasks,
                   const tsk_decode_image *__restrict__ images,
                   const tsk_row_start *__restrict__ rowtab, tsk_result *results, uint32_t one,
                   uint32_t top) {
     TableSource source{tasks, images, ntasks};
-    decode_body<MaxPayload, Stages, Paths, CW, G16>(source, rowtab, results, one, top);
+    decode_body<MaxPayload, Stages, Paths, CW, G16, NR>(source, rowtab, results, one, top);
 }
 
 // A serving batch: the requests arrive in the parameter block.
@@ -909,7 +1032,7 @@ __global__ void __launch_bounds__(threads_of(CW), MinBlocks)
                  const tsk_row_start *__restrict__ rowtab, tsk_result *results, uint32_t one,
                  uint32_t top) {
     ServeSource source{&batch, archives, batch.ntasks, 0};
-    decode_body<MaxPayload, Stages, Paths, CW, G16>(source, rowtab, results, one, top);
+    decode_body<MaxPayload, Stages, Paths, CW, G16, 0>(source, rowtab, results, one, top);
 }
 
 using KernelFn = void (*)(const tsk_decode_task *, uint32_t, const tsk_decode_image *,
@@ -926,9 +1049,9 @@ struct Variant {
 // plan's kernel carries only the code (and registers) it needs. The plain uint16 path, the
 // headline one, comes in four shapes (consumer warps x columns per lane) for the tuner.
 template <uint32_t MaxPayload, uint32_t Stages, uint32_t Paths, uint32_t CW = 8,
-          uint32_t G16 = 8, uint32_t MinBlocks = 3>
+          uint32_t G16 = 8, uint32_t MinBlocks = 3, uint32_t NR = 0>
 Variant make() {
-    return {decode_kernel<MaxPayload, Stages, Paths, CW, G16, MinBlocks>,
+    return {decode_kernel<MaxPayload, Stages, Paths, CW, G16, MinBlocks, NR>,
             sizeof(Shared<MaxPayload, Stages>), threads_of(CW)};
 }
 
@@ -959,6 +1082,14 @@ Variant select(uint32_t paths, uint32_t shape) {
                 return make<8192, 4, kU16 | kPlain, 4, 32, 3>();
             case 7:
                 return make<8192, 4, kU16 | kPlain, 4, 32, 4>();
+            case 8:
+                return make<8192, 4, kU16 | kPlain, 4, 16, 5, 1>();
+            case 9:
+                return make<8192, 4, kU16 | kPlain, 4, 16, 4, 2>();
+            case 10:
+                return make<8192, 4, kU16 | kPlain, 4, 16, 5, 2>();
+            case 11:
+                return make<8192, 4, kU16 | kPlain, 4, 8, 5, 2>();
             default:
                 return make<8192, 4, kU16 | kPlain, 8, 8, 4>();
             }
