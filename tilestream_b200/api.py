@@ -177,9 +177,10 @@ class ImageMetadata:
         addr = N.lib().ts_metadata_segments(self.handle)
         return np.frombuffer((C.c_uint8 * (n * 24)).from_address(addr), SEGMENT_DTYPE).copy()
 
-    def __del__(self):
+    def __del__(self, _lib=N.lib):
+        # _lib is bound at definition: module globals may already be gone at interpreter exit.
         if getattr(self, "handle", None):
-            N.lib().ts_metadata_destroy(self.handle)
+            _lib().ts_metadata_destroy(self.handle)
             self.handle = None
 
 

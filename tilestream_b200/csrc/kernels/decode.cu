@@ -38,9 +38,10 @@ namespace {
 
 constexpr uint32_t kFull = 0xffffffffu;
 
-// Threads of a CTA with CW consumer warps and the producer warp.
-constexpr uint32_t threads_of(uint32_t cw) {
-    return cw * 32 + 32;
+// Threads of a CTA with CW consumer warps and, unless the groups stage their own tiles, the
+// producer warp.
+constexpr uint32_t threads_of(uint32_t cw, bool self = false) {
+    return cw * 32 + (self ? 0 : 32);
 }
 
 enum : uint32_t { kStageOk = 0, kStageSkip = 1, kStageMalformed = 2 };
@@ -116,13 +117,14 @@ struct Ctx {
     uint32_t w, row0, row1, col0, col1;
     bool full;         // TSK_FULL: whole rows of a class width, 16-byte-aligned rows
     uint32_t one, top; // runtime constants 1 and 0x80000000 (see Pipes)
+    uint32_t slot;     // this warp's index among the warps that share the tile
 };
 
 // Pipe balance. On this SM the integer ALU pipe (logic, shifts, adds) and the FMA pipe
 // (integer multiply-add) each run at half the issue rate, and the uint16 decode is ALU-bound.
 // Additions written as multiply-adds by a runtime 1 (a kernel argument the compiler cannot
-// fold) execute on the FMA pipe instead, and so do the inverse zigzag's shifts, written as
-// multiplies by runtime powers of two (unzig16).
+// fold) execute on the FMA pipe instead, and so does the inverse zigzag's sign mask, a high
+// product (unzig16).
 struct Pipes {
     uint32_t one; // 1
     uint32_t top; // 0x80000000
@@ -134,17 +136,18 @@ __device__ __forceinline__ uint32_t fma_add(uint32_t a, uint32_t b, const Pipes 
     return d;
 }
 
-// Inverse zigzag of the item whose lowest bit is bit `at` of w, from the multiplier
-// m = 2^(31 - at) (0 for an empty row): the magnitude (w >> (at + 1)) & mh and the sign bit
-// moved to bit 31 are products on the FMA pipe (the multipliers are runtime values, so the
-// compiler keeps them as multiplies); the sign mask is an arithmetic shift and the combination
-// one logic op, both on the ALU pipe. Exact in the low 16 bits, which is all a uint16 sum uses.
-__device__ __forceinline__ uint32_t unzig16(uint32_t w, uint32_t m, uint32_t mh) {
-    uint32_t h, lo;
-    asm("mul.hi.u32 %0, %1, %2;" : "=r"(h) : "r"(w), "r"(m));
-    asm("mul.lo.u32 %0, %1, %2;" : "=r"(lo) : "r"(w), "r"(m));
-    const uint32_t sign = static_cast<uint32_t>(static_cast<int32_t>(lo) >> 31);
-    return (h & mh) ^ sign;
+// Inverse zigzag of the b-bit item whose lowest bit is bit `at` of x, given the rotation
+// amount at + 1: the rotation brings the magnitude bits (z >> 1) to bit 0 and the item's low bit
+// (the sign of the delta) to bit 31. The sign mask -(z & 1) is then the high word of the signed
+// product r * 2 (a multiply-add on the FMA pipe; `two` is 0 for an empty row, whose items are
+// all zero), and one logic op masks the magnitude (mh = 2^(b-1) - 1) and applies the sign:
+// z/2 or -(z/2) - 1. Exact in the low 16 bits, which is all a uint16 sum uses.
+__device__ __forceinline__ uint32_t unzig16(uint32_t x, uint32_t amount, uint32_t mh,
+                                            uint32_t two) {
+    const uint32_t r = __funnelshift_r(x, x, amount);
+    uint32_t sign;
+    asm("mul.hi.s32 %0, %1, %2;" : "=r"(sign) : "r"(r), "r"(two));
+    return (r & mh) ^ sign;
 }
 
 // The 64-bit window of the packed words that starts at the bit of item `first` of a row (item c
@@ -181,10 +184,11 @@ __device__ __forceinline__ void terms(const uint32_t *packed, uint32_t c0, uint3
                                       const Pipes &pipes, uint32_t (&t)[G]) {
     if constexpr (!F32) {
         // uint16, b <= 16: four residuals per 64-bit window. An empty row (b = 0) has no packed
-        // words: its multipliers are zero, so every term is zero whatever the window holds.
-        const uint32_t mh = low_mask(b) >> 1;           // the magnitude bits of a zigzag value
-        const uint32_t m0 = b != 0 ? pipes.top : 0u;    // 2^31: the item at bit 0
-        const uint32_t m1 = b != 0 ? pipes.top >> b : 0u; // 2^(31 - b): the item at bit b
+        // words: its magnitude mask and sign multiplier are zero, so every term is zero whatever
+        // the window holds.
+        const uint32_t mh = low_mask(b) >> 1;       // the magnitude bits of a zigzag value
+        const uint32_t two = b != 0 ? 2u * pipes.one : 0u;
+        const uint32_t a1 = b + 1;                  // rotation of the item at bit b
 #pragma unroll
         for (uint32_t q = 0; q < G; q += 4) {
             uint32_t x0, x1;
@@ -198,10 +202,10 @@ __device__ __forceinline__ void terms(const uint32_t *packed, uint32_t c0, uint3
             // Items q, q + 1 lie in x0 (2b <= 32 bits) and items q + 2, q + 3 in the word that
             // starts 2b bits later. Inverse zigzag as an unsigned delta: z/2 or -(z/2) - 1.
             const uint32_t y0 = __funnelshift_rc(x0, x1, 2 * b);
-            t[q] = unzig16(x0, m0, mh);
-            t[q + 1] = unzig16(x0, m1, mh);
-            t[q + 2] = unzig16(y0, m0, mh);
-            t[q + 3] = unzig16(y0, m1, mh);
+            t[q] = unzig16(x0, 1u, mh, two);
+            t[q + 1] = unzig16(x0, a1, mh, two);
+            t[q + 2] = unzig16(y0, 1u, mh, two);
+            t[q + 3] = unzig16(y0, a1, mh, two);
         }
     } else {
         // FP32 words, b <= 32: two residuals per 64-bit window.
@@ -314,8 +318,7 @@ __device__ __forceinline__ void store(const Ctx &x, uint8_t *line, const uint8_t
             if constexpr (G >= 8) {
 #pragma unroll
                 for (uint32_t k = 0; k < G / 2; k += 4) {
-                    *reinterpret_cast<uint4 *>(dst + 2 * k) =
-                        make_uint4(p[k], p[k + 1], p[k + 2], p[k + 3]);
+                    st_global_v4(dst + 2 * k, p[k], p[k + 1], p[k + 2], p[k + 3]);
                 }
             } else {
                 *reinterpret_cast<uint2 *>(dst) = make_uint2(p[0], p[1]);
@@ -332,6 +335,15 @@ __device__ __forceinline__ void store(const Ctx &x, uint8_t *line, const uint8_t
     }
 }
 
+// a * gate + b on the FMA pipe: with gate 1 (the runtime one) the sum, with gate 0 just b. Used
+// where a lane conditionally adds a neighbour's value, so that no branch is needed (the
+// compiler cannot predicate an inline-asm statement and would branch around it).
+__device__ __forceinline__ uint32_t gated_add(uint32_t a, uint32_t gate, uint32_t b) {
+    uint32_t d;
+    asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(gate), "r"(b));
+    return d;
+}
+
 // Decodes rows [row0, row1) of one staged tile with the CW consumer warps; LW lanes per row.
 // Full: the tile's width is G * LW (or twice that for FP32 256-wide rows) and every column is
 // written to aligned rows, so no per-group bounds or alignment checks are needed.
@@ -340,7 +352,8 @@ __device__ void decode_rows(const Ctx &x, const uint32_t *payload, const uint16_
                             uint32_t mode) {
     constexpr uint32_t kRowsPerWarp = 32 / LW;
     constexpr uint32_t kSpan = G * LW;
-    const uint32_t warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    // CW here: the warps that share the tile; warp: this warp's slot among them.
+    const uint32_t warp = CW == 1 ? 0u : x.slot, lane = threadIdx.x % 32;
     const uint32_t sub = lane % LW;
     const uint32_t w = x.w;
     const uint32_t passes = (x.col1 + kSpan - 1) / kSpan;
@@ -425,8 +438,11 @@ __device__ void decode_rows(const Ctx &x, const uint32_t *payload, const uint16_
 #pragma unroll
                 for (uint32_t d = 1; d < LW; d <<= 1) {
                     const uint32_t other = __shfl_up_sync(kFull, inclusive, d, LW);
-                    if (sub >= d) {
-                        inclusive = add(other, inclusive);
+                    // Branch-free conditional add (see gated_add).
+                    if constexpr (F32) {
+                        inclusive ^= sub >= d ? other : 0u;
+                    } else {
+                        inclusive = gated_add(other, sub >= d ? x.one : 0u, inclusive);
                     }
                 }
                 const uint32_t before = add(carry, uncombine<F32>(inclusive, total));
@@ -468,19 +484,29 @@ __device__ void decode_rows(const Ctx &x, const uint32_t *payload, const uint16_
 // Predictive uint16 rows. The class width G * LW covers every uint16 row (64, 128 or 256), so
 // a row is one pass of its LW lanes: no pass loop and no carry between passes. Each lane
 // decodes NR rows at once (rows r, r + R, ... with R = CW * 32 / LW), their steps interleaved so
-// that one row's shuffle scan and window loads overlap the other rows' arithmetic.
-template <uint32_t CW, uint32_t G, uint32_t LW, bool Cal, bool Full, uint32_t NR>
+// that one row's shuffle scan and window loads overlap the other rows' arithmetic. The inner
+// loop has no branches: the scan's conditional adds are gated multiply-adds, and AllLive (every
+// row of every iteration exists: the common whole-tile case) drops the per-row checks.
+template <uint32_t CW, uint32_t G, uint32_t LW, bool Cal, bool Full, uint32_t NR, bool AllLive>
 __device__ __forceinline__ void predict_rows_u16(const Ctx &x, const uint32_t *payload,
                                                  const uint16_t *rows) {
     constexpr uint32_t kRowsPerWarp = 32 / LW;
     constexpr uint32_t kStride = CW * kRowsPerWarp;
     constexpr uint32_t H = G / 2;
-    const uint32_t warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    constexpr uint32_t kSteps = LW == 1 ? 0 : LW == 2 ? 1 : LW == 4 ? 2 : LW == 8 ? 3 : LW == 16 ? 4 : 5;
+    // CW here: the warps that share the tile; warp: this warp's slot among them.
+    const uint32_t warp = CW == 1 ? 0u : x.slot, lane = threadIdx.x % 32;
     const uint32_t sub = lane % LW;
     const uint32_t c0 = sub * G;
     const uint32_t w = x.w;
     const Pipes pipes{x.one, x.top};
     auto add = [&pipes](uint32_t a, uint32_t b) { return fma_add(a, b, pipes); };
+    // gate[j]: 1 when this lane takes the value 2^j lanes to its left in scan step j.
+    uint32_t gate[kSteps > 0 ? kSteps : 1];
+#pragma unroll
+    for (uint32_t j = 0; j < kSteps; ++j) {
+        gate[j] = sub >= (1u << j) ? x.one : 0u;
+    }
     auto prefetch_maps = [&](uint32_t row) {
         if constexpr (Cal) {
             if (row < x.row1 && c0 < x.col1 && c0 + G > x.col0) {
@@ -515,7 +541,7 @@ __device__ __forceinline__ void predict_rows_u16(const Ctx &x, const uint32_t *p
 #pragma unroll
         for (uint32_t n = 0; n < NR; ++n) {
             const uint32_t r = base + n * kStride + lane / LW;
-            live[n] = r < x.row1;
+            live[n] = AllLive || r < x.row1;
             if constexpr (Cal) {
                 prefetch_maps(r + NR * kStride);
             }
@@ -545,18 +571,16 @@ __device__ __forceinline__ void predict_rows_u16(const Ctx &x, const uint32_t *p
             inclusive[n] = total[n];
         }
 #pragma unroll
-        for (uint32_t d = 1; d < LW; d <<= 1) {
+        for (uint32_t j = 0; j < kSteps; ++j) {
 #pragma unroll
             for (uint32_t n = 0; n < NR; ++n) {
-                const uint32_t other = __shfl_up_sync(kFull, inclusive[n], d, LW);
-                if (sub >= d) {
-                    inclusive[n] = add(other, inclusive[n]);
-                }
+                const uint32_t other = __shfl_up_sync(kFull, inclusive[n], 1u << j, LW);
+                inclusive[n] = gated_add(other, gate[j], inclusive[n]);
             }
         }
 #pragma unroll
         for (uint32_t n = 0; n < NR; ++n) {
-            if (live[n]) {
+            if (AllLive || live[n]) {
                 const uint32_t before = add(carry[n], inclusive[n] - total[n]);
                 const uint32_t mid = add(before, t[n][H - 1]);
                 uint32_t v[G];
@@ -581,10 +605,13 @@ __device__ __forceinline__ void decode_class(const Ctx &x, const uint32_t *paylo
                                              const uint16_t *rows, uint32_t mode) {
     if constexpr (!F32 && NR != 0) {
         if (mode == TSK_PREDICT) {
-            if (x.full) {
-                predict_rows_u16<CW, G, LW, Cal, true, NR>(x, payload, rows);
+            constexpr uint32_t kRowsPerIteration = NR * CW * (32 / LW);
+            if (x.full && (x.row1 - x.row0) % kRowsPerIteration == 0) {
+                predict_rows_u16<CW, G, LW, Cal, true, NR, true>(x, payload, rows);
+            } else if (x.full) {
+                predict_rows_u16<CW, G, LW, Cal, true, NR, false>(x, payload, rows);
             } else {
-                predict_rows_u16<CW, G, LW, Cal, false, NR>(x, payload, rows);
+                predict_rows_u16<CW, G, LW, Cal, false, NR, false>(x, payload, rows);
             }
             return;
         }
@@ -850,21 +877,138 @@ __device__ void stage_task(Sh &sh, uint32_t s, const tsk_decode_task &t, const S
     mbar_arrive(&sh.full[s]);
 }
 
+// Decodes the tile staged in stage s with the RW warps of this thread's group (slot: this
+// warp's index in it), then writes the tile's result-record updates (lead thread). Release: the
+// stage is handed back through its empty barrier (producer-warp mode); self-staging groups
+// reuse their stages themselves.
+template <uint32_t Paths, uint32_t RW, uint32_t G16, uint32_t NR, bool Release, typename Sh,
+          typename Source>
+__device__ __forceinline__ void consume_tile(Sh &sh, uint32_t s, const Source &source,
+                                             tsk_result *results, uint32_t one, uint32_t top,
+                                             bool lead, uint32_t slot, uint32_t group) {
+    const uint32_t lane = threadIdx.x % 32;
+    const StageHeader &h = sh.header[s];
+    const tsk_decode_task t = h.task;
+    const uint32_t state = h.state, hmode = h.mode;
+    const uint32_t *payload = reinterpret_cast<const uint32_t *>(sh.payload[s] + h.shift);
+    const bool f32 = (t.flags & TSK_F32) != 0;
+    const bool calibrated = (t.flags & TSK_CALIBRATED) != 0;
+    const bool trusted = (t.flags & TSK_TRUSTED) != 0;
+    bool ok = state == kStageOk;
+    if (trusted && ok && hmode == TSK_PREDICT) {
+        if (lead) {
+            sh.valid[s] = walk_rows(payload, h.words, t.width, t.height, f32, sh.rows[s]);
+        }
+        if constexpr (RW == 1) {
+            __syncwarp();
+        } else {
+            named_sync(1 + group, RW * 32);
+        }
+        ok = sh.valid[s] != 0;
+    }
+    if (ok) {
+        Ctx x;
+        x.out = reinterpret_cast<uint8_t *>(t.dst);
+        x.pitch = t.pitch;
+        x.w = t.width;
+        x.row0 = t.row0;
+        x.row1 = t.row1;
+        x.col0 = t.col0;
+        x.col1 = t.col1;
+        x.full = (t.flags & TSK_FULL) != 0;
+        x.one = one;
+        x.top = top;
+        x.slot = slot;
+        x.omap = x.gmap = nullptr;
+        x.opitch = x.gpitch = 0;
+        x.offset = 0.0f;
+        x.gain = 1.0f;
+        if (calibrated) {
+            x.offset = h.offset;
+            x.gain = h.gain;
+            x.opitch = h.opitch;
+            x.gpitch = h.gpitch;
+            x.omap = reinterpret_cast<const uint8_t *>(h.omap);
+            x.gmap = reinterpret_cast<const uint8_t *>(h.gmap);
+        }
+        const uint16_t *rows = sh.rows[s];
+        if constexpr ((Paths & kU16) && (Paths & kPlain)) {
+            if (!f32 && !calibrated) {
+                decode_tile<RW, G16, false, false, NR>(x, payload, rows, hmode);
+            }
+        }
+        if constexpr ((Paths & kF32) && (Paths & kPlain)) {
+            if (f32 && !calibrated) decode_tile<RW, G16, true, false, NR>(x, payload, rows, hmode);
+        }
+        if constexpr ((Paths & kU16) && (Paths & kCal)) {
+            if (!f32 && calibrated) decode_tile<RW, G16, false, true, NR>(x, payload, rows, hmode);
+        }
+        if constexpr ((Paths & kF32) && (Paths & kCal)) {
+            if (f32 && calibrated) decode_tile<RW, G16, true, true, NR>(x, payload, rows, hmode);
+        }
+    }
+    if constexpr (Release) {
+        __syncwarp();
+        if (lane == 0) {
+            mbar_arrive(&sh.empty[s]);
+        }
+    }
+    if (lead) {
+        bool counted = false;
+        if constexpr (Source::kTrusted) {
+            if (trusted) {
+                counted = true;
+                const tsk_decode_image &im = source.image(t.image);
+                if (state == kStageMalformed || (state == kStageOk && !ok)) {
+                    fail(results, t.image, 5u); // malformed_data
+                }
+                // Completion count: the last task of the image writes the final record.
+                __threadfence();
+                const uint32_t done = atomicAdd(&results[t.image].reserved, 1u);
+                if (done + 1 == im.tile_count) {
+                    __threadfence();
+                    uint32_t status =
+                        *reinterpret_cast<volatile uint32_t *>(&results[t.image].status);
+                    const uint32_t produced =
+                        reinterpret_cast<const volatile tsk_result *>(im.encoder_result)
+                            ->status;
+                    if (produced != 0) {
+                        status = produced;
+                    }
+                    results[t.image].reserved = 0;
+                    results[t.image].bytes_written = status == 0 ? im.result_bytes : 0;
+                    results[t.image].status = status;
+                }
+            }
+        }
+        if (!counted && (t.flags & TSK_FIRST)) {
+            results[t.image].status = 0;
+            results[t.image].reserved = 0;
+            results[t.image].bytes_written = source.result_bytes(t);
+        }
+    }
+}
+
 // The persistent loop over a task source: CW consumer warps, G16 columns per lane for uint16
-// rows.
+// rows. The consumers form CW / RW groups of RW warps; group g decodes this CTA's tiles g,
+// g + CW / RW, ..., each of its warps a slice of the tile's rows, and the group releases the
+// tile's stage. RW = CW: every warp works on every tile; smaller groups run a tile's set-up
+// fewer times per tile.
 template <uint32_t MaxPayload, uint32_t Stages, uint32_t Paths, uint32_t CW, uint32_t G16,
-          uint32_t NR, typename Source>
+          uint32_t NR, uint32_t RW, typename Source>
 __device__ __forceinline__ void decode_body(Source &source, const tsk_row_start *rowtab,
                                             tsk_result *results, uint32_t one, uint32_t top) {
     using Sh = Shared<MaxPayload, Stages>;
     constexpr uint32_t kConsumers = CW * 32;
+    constexpr uint32_t kGroups = CW / RW;
+    static_assert(CW % RW == 0, "groups of equal size");
     extern __shared__ __align__(128) uint8_t smem_raw[];
     Sh &sh = *reinterpret_cast<Sh *>(smem_raw);
     const uint32_t warp = threadIdx.x / 32, lane = threadIdx.x % 32;
     if (threadIdx.x == 0) {
         for (uint32_t s = 0; s < Stages; ++s) {
             mbar_init(&sh.full[s], 1);
-            mbar_init(&sh.empty[s], CW);
+            mbar_init(&sh.empty[s], RW);
         }
         fence_barrier_init();
     }
@@ -895,8 +1039,12 @@ __device__ __forceinline__ void decode_body(Source &source, const tsk_row_start 
             if (i + 1 < mine) {
                 next = source.task(blockIdx.x + (i + 1) * gridDim.x);
             }
-            if (i >= Stages && !mbar_wait(&sh.empty[s], ((i / Stages) - 1) & 1u)) {
-                return; // consumers stopped; they have reported the timeout
+            if (i >= Stages) {
+                const bool freed = RW < CW ? mbar_wait_backoff(&sh.empty[s], ((i / Stages) - 1) & 1u)
+                                           : mbar_wait(&sh.empty[s], ((i / Stages) - 1) & 1u);
+                if (!freed) {
+                    return; // consumers stopped; they have reported the timeout
+                }
             }
             stage_task(sh, s, t, source, rowtab);
             t = next;
@@ -907,105 +1055,99 @@ __device__ __forceinline__ void decode_body(Source &source, const tsk_row_start 
     // Consumers write outputs and result records, which the stream's previous grid may still
     // be reading or writing.
     griddep_wait();
-    for (uint32_t i = 0; i < mine; ++i) {
+    // The thread that walks trusted rows and writes result records for this group's tiles.
+    const uint32_t group = warp / RW, slot = warp % RW;
+    const bool lead = lane == 0 && slot == 0;
+    for (uint32_t i = group; i < mine; i += kGroups) {
         const uint32_t s = i % Stages;
         if (!mbar_wait(&sh.full[s], (i / Stages) & 1u)) {
-            if (threadIdx.x == 0) {
+            if (lead) {
                 fail(results, source.image_of(blockIdx.x + i * gridDim.x), 9u); // cuda_error
             }
             return;
         }
-        const StageHeader &h = sh.header[s];
-        const tsk_decode_task t = h.task;
-        const uint32_t state = h.state, hmode = h.mode;
-        const uint32_t *payload = reinterpret_cast<const uint32_t *>(sh.payload[s] + h.shift);
-        const bool f32 = (t.flags & TSK_F32) != 0;
-        const bool calibrated = (t.flags & TSK_CALIBRATED) != 0;
-        const bool trusted = (t.flags & TSK_TRUSTED) != 0;
-        bool ok = state == kStageOk;
-        if (trusted && ok && hmode == TSK_PREDICT) {
-            if (threadIdx.x == 0) {
-                sh.valid[s] = walk_rows(payload, h.words, t.width, t.height, f32, sh.rows[s]);
-            }
-            named_sync(1, kConsumers);
-            ok = sh.valid[s] != 0;
+        consume_tile<Paths, RW, G16, NR, true>(sh, s, source, results, one, top, lead, slot,
+                                               group);
+    }
+}
+
+// The persistent loop without a producer warp: CW consumer warps in CW / RW groups, each group
+// staging its own tiles into two stages of its own (stages 2g and 2g + 1) and decoding them in
+// turn, so no group waits on another's progress. Group g takes this CTA's tiles g, g + CW / RW,
+// ...; its k-th tile uses stage 2g + (k & 1). After a tile is decoded the group synchronises,
+// and the group's lead thread restages that stage with the group's tile after next while the
+// other stage, already loaded, is decoded. Each lead thread prefetches the task record of the
+// tile it will stage next. Stages must equal 2 * CW / RW.
+template <uint32_t MaxPayload, uint32_t Stages, uint32_t Paths, uint32_t CW, uint32_t G16,
+          uint32_t NR, uint32_t RW, typename Source>
+__device__ __forceinline__ void decode_body_self(Source &source, const tsk_row_start *rowtab,
+                                                 tsk_result *results, uint32_t one,
+                                                 uint32_t top) {
+    using Sh = Shared<MaxPayload, Stages>;
+    constexpr uint32_t kGroups = CW / RW;
+    static_assert(CW % RW == 0 && Stages == 2 * kGroups, "two stages per group");
+    extern __shared__ __align__(128) uint8_t smem_raw[];
+    Sh &sh = *reinterpret_cast<Sh *>(smem_raw);
+    const uint32_t warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const uint32_t group = warp / RW, slot = warp % RW;
+    const bool lead = lane == 0 && slot == 0;
+    if (threadIdx.x == 0) {
+        for (uint32_t s = 0; s < Stages; ++s) {
+            mbar_init(&sh.full[s], 1);
         }
-        if (ok) {
-            Ctx x;
-            x.out = reinterpret_cast<uint8_t *>(t.dst);
-            x.pitch = t.pitch;
-            x.w = t.width;
-            x.row0 = t.row0;
-            x.row1 = t.row1;
-            x.col0 = t.col0;
-            x.col1 = t.col1;
-            x.full = (t.flags & TSK_FULL) != 0;
-            x.one = one;
-            x.top = top;
-            x.omap = x.gmap = nullptr;
-            x.opitch = x.gpitch = 0;
-            x.offset = 0.0f;
-            x.gain = 1.0f;
-            if (calibrated) {
-                x.offset = h.offset;
-                x.gain = h.gain;
-                x.opitch = h.opitch;
-                x.gpitch = h.gpitch;
-                x.omap = reinterpret_cast<const uint8_t *>(h.omap);
-                x.gmap = reinterpret_cast<const uint8_t *>(h.gmap);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        griddep_launch_dependents();
+    }
+    const uint32_t ntasks = source.ntasks;
+    const uint32_t mine = blockIdx.x < ntasks ? (ntasks - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+    // This group's k-th tile is the CTA's tile group + k * kGroups.
+    const uint32_t count = group < mine ? (mine - 1 - group) / kGroups + 1 : 0;
+    auto queue_index = [&](uint32_t k) { return blockIdx.x + (group + k * kGroups) * gridDim.x; };
+    auto group_sync = [&]() {
+        if constexpr (RW == 1) {
+            __syncwarp();
+        } else {
+            named_sync(1 + group, RW * 32);
+        }
+    };
+    // Task records are the plan's (or the server's) own tables, written before any launch, so
+    // they are read before waiting for the stream's previous grid; payloads, outputs and
+    // results are touched after.
+    tsk_decode_task next{};
+    if (lead && count > 0) {
+        next = source.task(queue_index(0));
+    }
+    griddep_wait();
+    if (lead) {
+        for (uint32_t k = 0; k < 2 && k < count; ++k) {
+            const tsk_decode_task t = next;
+            if (k + 1 < count) {
+                next = source.task(queue_index(k + 1));
             }
-            const uint16_t *rows = sh.rows[s];
-            if constexpr ((Paths & kU16) && (Paths & kPlain)) {
-                if (!f32 && !calibrated) {
-                    decode_tile<CW, G16, false, false, NR>(x, payload, rows, hmode);
+            stage_task(sh, 2 * group + k, t, source, rowtab);
+        }
+    }
+    for (uint32_t k = 0; k < count; ++k) {
+        const uint32_t s = 2 * group + (k & 1u);
+        if (!mbar_wait(&sh.full[s], (k >> 1) & 1u)) {
+            if (lead) {
+                fail(results, source.image_of(queue_index(k)), 9u); // cuda_error
+            }
+            return;
+        }
+        consume_tile<Paths, RW, G16, NR, false>(sh, s, source, results, one, top, lead, slot,
+                                                group);
+        if (k + 2 < count) {
+            group_sync(); // every warp of the group is done with stage s
+            if (lead) {
+                const tsk_decode_task t = next;
+                if (k + 3 < count) {
+                    next = source.task(queue_index(k + 3));
                 }
-            }
-            if constexpr ((Paths & kF32) && (Paths & kPlain)) {
-                if (f32 && !calibrated) decode_tile<CW, G16, true, false, NR>(x, payload, rows, hmode);
-            }
-            if constexpr ((Paths & kU16) && (Paths & kCal)) {
-                if (!f32 && calibrated) decode_tile<CW, G16, false, true, NR>(x, payload, rows, hmode);
-            }
-            if constexpr ((Paths & kF32) && (Paths & kCal)) {
-                if (f32 && calibrated) decode_tile<CW, G16, true, true, NR>(x, payload, rows, hmode);
-            }
-        }
-        __syncwarp();
-        if (lane == 0) {
-            mbar_arrive(&sh.empty[s]);
-        }
-        if (threadIdx.x == 0) {
-            bool counted = false;
-            if constexpr (Source::kTrusted) {
-                if (trusted) {
-                    counted = true;
-                    const tsk_decode_image &im = source.image(t.image);
-                    if (state == kStageMalformed || (state == kStageOk && !ok)) {
-                        fail(results, t.image, 5u); // malformed_data
-                    }
-                    // Completion count: the last task of the image writes the final record.
-                    __threadfence();
-                    const uint32_t done = atomicAdd(&results[t.image].reserved, 1u);
-                    if (done + 1 == im.tile_count) {
-                        __threadfence();
-                        uint32_t status =
-                            *reinterpret_cast<volatile uint32_t *>(&results[t.image].status);
-                        const uint32_t produced =
-                            reinterpret_cast<const volatile tsk_result *>(im.encoder_result)
-                                ->status;
-                        if (produced != 0) {
-                            status = produced;
-                        }
-                        results[t.image].reserved = 0;
-                        results[t.image].bytes_written = status == 0 ? im.result_bytes : 0;
-                        results[t.image].status = status;
-                    }
-                }
-            }
-            if (!counted && (t.flags & TSK_FIRST)) {
-                results[t.image].status = 0;
-                results[t.image].reserved = 0;
-                results[t.image].bytes_written = source.result_bytes(t);
+                stage_task(sh, s, t, source, rowtab);
             }
         }
     }
@@ -1013,14 +1155,20 @@ __device__ __forceinline__ void decode_body(Source &source, const tsk_row_start 
 
 // A planned queue (every plan and mixed batch); MinBlocks resident CTAs per SM.
 template <uint32_t MaxPayload, uint32_t Stages, uint32_t Paths, uint32_t CW, uint32_t G16,
-          uint32_t MinBlocks, uint32_t NR>
-__global__ void __launch_bounds__(threads_of(CW), MinBlocks)
+          uint32_t MinBlocks, uint32_t NR, uint32_t RW, bool Self>
+__global__ void __launch_bounds__(threads_of(CW, Self), MinBlocks)
     decode_kernel(const tsk_decode_task *__restrict__ tasks, uint32_t ntasks,
                   const tsk_decode_image *__restrict__ images,
                   const tsk_row_start *__restrict__ rowtab, tsk_result *results, uint32_t one,
                   uint32_t top) {
     TableSource source{tasks, images, ntasks};
-    decode_body<MaxPayload, Stages, Paths, CW, G16, NR>(source, rowtab, results, one, top);
+    if constexpr (Self) {
+        decode_body_self<MaxPayload, Stages, Paths, CW, G16, NR, RW>(source, rowtab, results, one,
+                                                                      top);
+    } else {
+        decode_body<MaxPayload, Stages, Paths, CW, G16, NR, RW>(source, rowtab, results, one,
+                                                                 top);
+    }
 }
 
 // A serving batch: the requests arrive in the parameter block.
@@ -1032,7 +1180,7 @@ __global__ void __launch_bounds__(threads_of(CW), MinBlocks)
                  const tsk_row_start *__restrict__ rowtab, tsk_result *results, uint32_t one,
                  uint32_t top) {
     ServeSource source{&batch, archives, batch.ntasks, 0};
-    decode_body<MaxPayload, Stages, Paths, CW, G16, 0>(source, rowtab, results, one, top);
+    decode_body<MaxPayload, Stages, Paths, CW, G16, 0, CW>(source, rowtab, results, one, top);
 }
 
 using KernelFn = void (*)(const tsk_decode_task *, uint32_t, const tsk_decode_image *,
@@ -1049,10 +1197,11 @@ struct Variant {
 // plan's kernel carries only the code (and registers) it needs. The plain uint16 path, the
 // headline one, comes in four shapes (consumer warps x columns per lane) for the tuner.
 template <uint32_t MaxPayload, uint32_t Stages, uint32_t Paths, uint32_t CW = 8,
-          uint32_t G16 = 8, uint32_t MinBlocks = 3, uint32_t NR = 0>
+          uint32_t G16 = 8, uint32_t MinBlocks = 3, uint32_t NR = 0, uint32_t RW = CW,
+          bool Self = false>
 Variant make() {
-    return {decode_kernel<MaxPayload, Stages, Paths, CW, G16, MinBlocks, NR>,
-            sizeof(Shared<MaxPayload, Stages>), threads_of(CW)};
+    return {decode_kernel<MaxPayload, Stages, Paths, CW, G16, MinBlocks, NR, RW, Self>,
+            sizeof(Shared<MaxPayload, Stages>), threads_of(CW, Self)};
 }
 
 // Shapes of the plain uint16 instance (consumer warps x uint16 columns per lane, stages,
@@ -1090,6 +1239,18 @@ Variant select(uint32_t paths, uint32_t shape) {
                 return make<8192, 4, kU16 | kPlain, 4, 16, 5, 2>();
             case 11:
                 return make<8192, 4, kU16 | kPlain, 4, 8, 5, 2>();
+            case 12:
+                return make<8192, 5, kU16 | kPlain, 4, 16, 4, 1, 1>();
+            case 13:
+                return make<8192, 4, kU16 | kPlain, 4, 16, 5, 1, 2>();
+            case 14:
+                return make<8192, 4, kU16 | kPlain, 4, 16, 5, 1, 2, true>();
+            case 15:
+                return make<8192, 4, kU16 | kPlain, 4, 16, 6, 1, 2, true>();
+            case 16:
+                return make<8192, 4, kU16 | kPlain, 4, 16, 4, 2, 2, true>();
+            case 17:
+                return make<8192, 8, kU16 | kPlain, 4, 16, 3, 1, 1, true>();
             default:
                 return make<8192, 4, kU16 | kPlain, 8, 8, 4>();
             }
@@ -1183,6 +1344,11 @@ extern "C" int tsk_decode_prepare(tsk_decode_config *config, uint32_t ntasks, in
     cudaError_t e = cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(v.smem));
     if (e != cudaSuccess) return e;
+    // The largest shared-memory carveout, so that occupancy is bounded by the instance's own
+    // needs and not by the default split between L1 and shared memory.
+    e = cudaFuncSetAttribute(v.fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             cudaSharedmemCarveoutMaxShared);
+    if (e != cudaSuccess) return e;
     if (sms == 0) {
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v.fn, v.threads, v.smem);
         if (e != cudaSuccess) return e;
@@ -1274,6 +1440,9 @@ extern "C" int tsk_serve_prepare(int all_u16, int device, uint32_t *grid) {
     const tsk::ServeVariant v = tsk::select_serve(all_u16 != 0);
     cudaError_t e = cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(v.smem));
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(v.fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             cudaSharedmemCarveoutMaxShared);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v.fn, v.threads, v.smem);

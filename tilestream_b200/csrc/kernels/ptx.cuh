@@ -61,6 +61,27 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
     return false;
 }
 
+// For a waiter with slack (the producer, stages ahead of its consumers): probes without a
+// suspend hint and sleeps between probes, so that a long wait costs few issue slots. Bounded
+// like mbar_wait (at most about 2^20 probes of at most ~1 us each).
+__device__ __forceinline__ bool mbar_wait_backoff(uint64_t *bar, uint32_t parity) {
+    constexpr uint32_t kLimit = 1u << 20;
+    for (uint32_t i = 0; i < kLimit; ++i) {
+        uint32_t done;
+        asm volatile("{\n\t.reg .pred p;\n\t"
+                     "mbarrier.try_wait.parity.acquire.cta.shared::cta.b64 p, [%1], %2;\n\t"
+                     "selp.u32 %0, 1, 0, p;\n\t}"
+                     : "=r"(done)
+                     : "r"(smem_addr(bar)), "r"(parity)
+                     : "memory");
+        if (done != 0) {
+            return true;
+        }
+        __nanosleep(256);
+    }
+    return false;
+}
+
 // Bulk copy of bytes (multiple of 16, both addresses 16-byte aligned) from global memory into
 // this CTA's shared memory; completion is signalled as transaction bytes on bar.
 __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes,
@@ -111,6 +132,14 @@ __device__ __forceinline__ void griddep_launch_dependents() {
 // Named barrier over a subset of the CTA's warps.
 __device__ __forceinline__ void named_sync(uint32_t id, uint32_t threads) {
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(threads) : "memory");
+}
+
+// 16-byte store to global memory (an evict-first hint measured slower). No memory clobber: the
+// kernel never reads what it stores.
+__device__ __forceinline__ void st_global_v4(void *p, uint32_t a, uint32_t b, uint32_t c,
+                                             uint32_t d) {
+    asm volatile("st.global.v4.b32 [%0], {%1, %2, %3, %4};" ::"l"(p), "r"(a), "r"(b), "r"(c),
+                 "r"(d));
 }
 
 __device__ __forceinline__ uint4 ld_nc_v4(const void *p) {

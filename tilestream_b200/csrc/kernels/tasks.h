@@ -102,7 +102,7 @@ typedef struct {
 // Kernel shapes of the plain uint16 decoder (consumer warps, columns per lane, stages and
 // resident CTAs per SM; listed in decode.cu). Other instances map odd shapes to 0 and even
 // shapes to 2.
-#define TSK_DECODE_SHAPES 12
+#define TSK_DECODE_SHAPES 18
 
 // One image to encode. 96 bytes.
 typedef struct __align__(16) {

@@ -51,9 +51,10 @@ class BatchPlan:
             raise RuntimeError(f"workspace_size: {st!r}")
         return n
 
-    def __del__(self):
+    def __del__(self, _lib=N.lib):
+        # _lib is bound at definition: module globals may already be gone at interpreter exit.
         if getattr(self, "handle", None):
-            N.lib().ts_plan_destroy(self.handle)
+            _lib().ts_plan_destroy(self.handle)
             self.handle = None
 
 
@@ -151,9 +152,10 @@ class MixedBatch:
         return {"tiles": s.tiles, "shape": s.shape, "grid": s.grid, "per_sm": s.per_sm,
                 "graph": bool(s.graph), "tuned_us": round(s.tuned_us, 2)}
 
-    def __del__(self):
+    def __del__(self, _lib=N.lib):
+        # _lib is bound at definition: module globals may already be gone at interpreter exit.
         if getattr(self, "handle", None):
-            N.lib().ts_mixed_batch_destroy(self.handle)
+            _lib().ts_mixed_batch_destroy(self.handle)
             self.handle = None
 
 
@@ -223,9 +225,10 @@ class Server:
         st = N.lib().ts_server_run(self.handle, arr, count, outcomes, C.byref(stats))
         return Status(st), outcomes, stats
 
-    def __del__(self):
+    def __del__(self, _lib=N.lib):
+        # _lib is bound at definition: module globals may already be gone at interpreter exit.
         if getattr(self, "handle", None):
-            N.lib().ts_server_destroy(self.handle)
+            _lib().ts_server_destroy(self.handle)
             self.handle = None
 
 
