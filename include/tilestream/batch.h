@@ -27,7 +27,14 @@ struct MixedOptions {
     // process and, when tune_cache names a file, across processes.
     bool autotune = false;
     const char *tune_cache = nullptr;
+    // A fixed kernel shape (0 .. decode_shape_count() - 1) instead of the default one, with the
+    // occupancy-derived grid; the autotuner is then not run. -1: the default shape. Used to
+    // check each shape's output and to measure shapes against each other.
+    std::int32_t shape = -1;
 };
+
+// The number of kernel shapes a MixedOptions::shape may name.
+[[nodiscard]] std::uint32_t decode_shape_count() noexcept;
 
 struct MixedStats {
     std::uint64_t tiles = 0;  // tasks in the device queue

@@ -137,7 +137,9 @@ typedef struct {
     uint32_t graph;         /* nonzero: executions replay a CUDA graph */
     uint32_t autotune;      /* nonzero: time candidate kernel shapes and grids at preparation */
     const char *tune_cache; /* file remembering tuned choices, or NULL */
+    int32_t shape;          /* a fixed kernel shape, 0 .. ts_decode_shape_count() - 1; -1: default */
 } ts_mixed_options;
+uint32_t ts_decode_shape_count(void);
 typedef struct {
     uint64_t tiles;
     uint32_t shape, grid, per_sm, graph;

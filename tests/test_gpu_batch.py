@@ -135,3 +135,43 @@ def test_mixed_batch_validation(cuda_ready, oracle_lib):
     assert cuda.prepare_mixed_batch(items, overlap, stream)[0] == Status.invalid_argument
     st, empty = cuda.prepare_mixed_batch([], results, stream)
     assert st == Status.success and empty.run(stream) == Status.success
+
+
+def plain_items(o, seeds, f32):
+    """Decompress and decode_roi items only (no calibration), uint16 only or uint16 + FP32."""
+    picked = [s for s in seeds if f32 or o.case(s)["type"] == 1]
+    items, keep, checks = build_items(o, picked)
+    kept = [(it, c) for it, c in zip(items, checks) if it[0] != cuda.Operation.decode_calibrate]
+    return [it for it, _ in kept], keep, [c for _, c in kept]
+
+
+def verify_plain(checks, results):
+    raw = host(results).view(np.uint64).reshape(-1, 2)
+    for k, (out, pitch, row_bytes, rh, want, nbytes) in enumerate(checks):
+        assert int(raw[k, 0]) == 0 and int(raw[k, 1]) == nbytes, k
+        got = host(out)[:pitch * rh].reshape(rh, pitch)
+        assert np.array_equal(np.ascontiguousarray(got[:, :row_bytes]), want), k
+        assert np.all(got[:, row_bytes:] == SENTINEL), k
+
+
+@pytest.mark.parametrize("f32", [False, True])
+def test_every_kernel_shape_matches_oracle(cuda_ready, oracle_lib, f32):
+    """Each kernel shape (MixedOptions.shape), forced in turn on plain batches - uint16 only, and
+    uint16 with FP32 - decodes every item to the oracle's words."""
+    torch = cuda_ready
+    stream = torch.cuda.current_stream()
+    items, keep, checks = plain_items(oracle_lib, list(range(13005000, 13005060)), f32)
+    assert any(op == cuda.Operation.decode_roi for op, _ in items)
+    for shape in range(cuda.decode_shape_count()):
+        results = device_bytes(16 * len(items), fill=0xFF)
+        for out, pitch, row_bytes, rh, want, nbytes in checks:
+            out.fill_(SENTINEL)
+        st, batch = cuda.prepare_mixed_batch(items, results, stream, shape=shape)
+        assert st == Status.success, (shape, st)
+        assert batch.stats()["shape"] == shape
+        assert batch.run(stream) == Status.success
+        torch.cuda.synchronize()
+        verify_plain(checks, results)
+    st, _ = cuda.prepare_mixed_batch(items, device_bytes(16 * len(items)), stream,
+                                     shape=cuda.decode_shape_count())
+    assert st == Status.invalid_argument

@@ -120,7 +120,8 @@ class MixedItem(C.Structure):
 
 
 class MixedOptions(C.Structure):
-    _fields_ = [("graph", u32), ("autotune", u32), ("tune_cache", C.c_char_p)]
+    _fields_ = [("graph", u32), ("autotune", u32), ("tune_cache", C.c_char_p),
+                ("shape", C.c_int32)]
 
 
 class MixedStats(C.Structure):
@@ -183,6 +184,7 @@ _SIGNATURES = {
     "ts_prepare_mixed_batch": (C.c_int, [C.POINTER(MixedItem), u64, ResultBuffer,
                                          C.POINTER(MixedOptions), C.POINTER(vp), vp]),
     "ts_run_mixed_batch": (C.c_int, [vp, vp]),
+    "ts_decode_shape_count": (u32, []),
     "ts_mixed_batch_stats": (C.c_int, [vp, C.POINTER(MixedStats)]),
     "ts_mixed_batch_destroy": (None, [vp]),
     "ts_server_create": (C.c_int, [C.POINTER(ServeOptions), C.POINTER(vp)]),

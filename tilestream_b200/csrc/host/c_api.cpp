@@ -360,6 +360,7 @@ extern "C" int ts_prepare_mixed_batch(const ts_mixed_item *items, uint64_t count
             o.graph = options->graph != 0;
             o.autotune = options->autotune != 0;
             o.tune_cache = options->tune_cache;
+            o.shape = options->shape;
         }
         auto holder = std::make_unique<ts_mixed_batch>();
         const ts::Status st = ts::cuda::prepare_mixed_batch(
@@ -373,6 +374,10 @@ extern "C" int ts_prepare_mixed_batch(const ts_mixed_item *items, uint64_t count
     } catch (...) {
         return code(ts::Status::resource_limit);
     }
+}
+
+extern "C" uint32_t ts_decode_shape_count(void) {
+    return ts::cuda::decode_shape_count();
 }
 
 extern "C" int ts_run_mixed_batch(const ts_mixed_batch *batch, void *stream) {

@@ -1080,7 +1080,10 @@ std::string tune_key(const detail::PlanState &p, int device) {
     for (char &c : key) {
         if (c == ' ') c = '_';
     }
-    return key + "/paths" + std::to_string(p.config.paths) + "/tasks2^" + std::to_string(order);
+    // The candidate set is part of the key, so that choices made among other shapes (an older
+    // library's cache file) are not replayed.
+    return key + "/paths" + std::to_string(p.config.paths) + "/tasks2^" + std::to_string(order) +
+           "/shapes" + std::to_string(TSK_DECODE_SHAPES);
 }
 
 void load_tune_cache(const char *path) {
@@ -1239,7 +1242,16 @@ Status prepare_mixed_batch(const MixedItem *items, std::uint64_t count, ResultBu
                 return st;
             }
             impl->results = reinterpret_cast<tsk_result *>(results.data);
-            if (options.autotune) {
+            if (options.shape >= static_cast<std::int32_t>(TSK_DECODE_SHAPES)) {
+                return Status::invalid_argument;
+            }
+            if (options.shape >= 0) {
+                plan.config.shape = static_cast<std::uint32_t>(options.shape);
+                const int e = tsk_decode_prepare(&plan.config, plan.task_count, plan.device);
+                if (e != 0) {
+                    return detail::cuda_failure("kernel shape", static_cast<cudaError_t>(e));
+                }
+            } else if (options.autotune) {
                 const char *cache = options.tune_cache != nullptr
                                         ? options.tune_cache
                                         : std::getenv("TILESTREAM_TUNE_CACHE");
@@ -1298,6 +1310,10 @@ Status run_mixed_batch(const MixedBatch &batch, cudaStream_t stream) noexcept {
         return detail::cuda_status(cudaGraphLaunch(impl->exec, stream), "cudaGraphLaunch");
     }
     return detail::cuda_status(enqueue_decode(p, impl->results, stream), "decode launch");
+}
+
+std::uint32_t decode_shape_count() noexcept {
+    return TSK_DECODE_SHAPES;
 }
 
 MixedStats mixed_batch_stats(const MixedBatch &batch) noexcept {

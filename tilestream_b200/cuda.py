@@ -159,13 +159,18 @@ class MixedBatch:
             self.handle = None
 
 
+def decode_shape_count() -> int:
+    return int(N.lib().ts_decode_shape_count())
+
+
 def prepare_mixed_batch(items, results, stream=None, graph=True, autotune=False,
-                        tune_cache=None):
-    """items: iterable of (Operation, BatchItem). Returns (Status, MixedBatch or None)."""
+                        tune_cache=None, shape=-1):
+    """items: iterable of (Operation, BatchItem). Returns (Status, MixedBatch or None).
+    shape >= 0 fixes the kernel shape (no tuning)."""
     items = list(items)
     arr = (N.MixedItem * max(1, len(items)))(*[N.MixedItem(int(op), it) for op, it in items])
     opts = N.MixedOptions(1 if graph else 0, 1 if autotune else 0,
-                          tune_cache.encode() if tune_cache else None)
+                          tune_cache.encode() if tune_cache else None, int(shape))
     h = C.c_void_p(0)
     st = N.lib().ts_prepare_mixed_batch(arr, len(items), _results(results), C.byref(opts),
                                         C.byref(h), stream_handle(stream))
