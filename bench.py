@@ -20,6 +20,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import statistics
 import sys
@@ -236,20 +237,27 @@ def run_ours(args, rank, world, device, torch, dist):
         st = cuda.decompress_async(step_plans[step % copies], wsb, step_recs, stream)
         assert st == Status.success, st
 
-    # One graph per rotation slot: the decode of that slot's three archives. The executors validate
-    # pointers with cudaPointerGetAttributes on the host, which global-mode capture rejects, so
-    # capture is relaxed (the validation runs once, at capture time).
-    graphs, capture_error = [], None
+    # CUDA graphs of the step: one per rotation slot (the decode of that slot's three archives),
+    # and one cycle graph holding the steps of every slot in order. Inside the cycle the decode
+    # kernels are programmatic dependents of one another, as consecutive executions in a stream
+    # are, so a step's launch overlaps the previous step's end; separate graph launches do not
+    # overlap. The executors validate pointers with cudaPointerGetAttributes on the host, which
+    # global-mode capture rejects, so capture is relaxed (the validation runs once, at capture).
+    graphs, cycle, capture_error = [], None, None
     try:
         for slot in range(copies):
             g = torch.cuda.CUDAGraph()
             with torch.cuda.graph(g, stream=stream, capture_error_mode="relaxed"):
                 enqueue(slot)
             graphs.append(g)
+        cycle = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(cycle, stream=stream, capture_error_mode="relaxed"):
+            for slot in range(copies):
+                enqueue(slot)
     except Exception as e:  # noqa: BLE001 - recorded in the JSON line, launches stay eager
         capture_error = str(e).splitlines()[0]
         print(f"graph capture failed, timing eager launches: {capture_error}", file=sys.stderr)
-        graphs = None
+        graphs, cycle = None, None
     torch.cuda.synchronize()
 
     def replay(i):
@@ -257,6 +265,18 @@ def run_ours(args, rank, world, device, torch, dist):
             graphs[i % copies].replay()
         else:
             enqueue(i % copies)
+
+    def run_steps(first, count):
+        """Steps first .. first + count - 1 (each one decode of its slot's three archives)."""
+        i, end = first, first + count
+        while i < end:
+            if cycle is not None and i % copies == 0 and end - i >= copies:
+                cycle.replay()
+                i += copies
+            else:
+                replay(i)
+                i += 1
+        return end
 
     # Correctness of the benchmarked outputs (one slot per shape).
     for s in shapes:
@@ -269,25 +289,43 @@ def run_ours(args, rank, world, device, torch, dist):
     r = results.cpu().numpy().view(np.uint64).reshape(3, 2)
     assert all(int(r[k, 0]) == 0 and int(r[k, 1]) == W * H * 2 for k in range(3)), r
 
-    for i in range(args.warmup):
-        replay(i)
+    step_index = run_steps(0, args.warmup)
     torch.cuda.synchronize()
-    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    # The timed region is K steps. It is repeated back to back until the repetitions span at
+    # least 0.2 s (so that clock samples cover it), each region bracketed by its own events;
+    # the reported time is the median region, with the spread beside it.
+    pilot0, pilot1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    pilot0.record(stream)
+    step_index = run_steps(step_index, args.steps)
+    pilot1.record(stream)
+    torch.cuda.synchronize()
+    pilot_ms = max(pilot0.elapsed_time(pilot1), 1e-3)
+    regions = int(min(args.max_regions, max(1, math.ceil(args.min_span_ms / pilot_ms))))
+    events = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(regions)]
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
     with ClockSampler(device) as clocks:
-        start.record(stream)
-        for i in range(args.steps):
-            replay(i)
-        end.record(stream)
+        for e0, e1 in events:
+            e0.record(stream)
+            step_index = run_steps(step_index, args.steps)
+            e1.record(stream)
         torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    ms = max_over_ranks(start.elapsed_time(end), world, dist, "cuda")
+    region_ms = sorted(e0.elapsed_time(e1) for e0, e1 in events)
+    median_ms = float(np.median(region_ms))
+    ms = max_over_ranks(median_ms, world, dist, "cuda")
     step_ms = ms / args.steps
     decoded_per_step = 3 * W * H * 2
     value = aggregate_gbs(decoded_per_step, args.steps, world, ms)
+    spread = {"regions": regions, "steps_per_region": args.steps,
+              "median_ms": round(median_ms, 5),
+              "p05_ms": round(float(np.percentile(region_ms, 5)), 5),
+              "p95_ms": round(float(np.percentile(region_ms, 95)), 5),
+              "min_ms": round(region_ms[0], 5), "max_ms": round(region_ms[-1], 5),
+              "span_ms": round(sum(region_ms), 2)}
 
     # Per-shape device time (outside the timed region, same method).
     per_shape = {}
@@ -340,7 +378,9 @@ def run_ours(args, rank, world, device, torch, dist):
                          " > 126 MB L2)",
                    "parallelism": f"replicas{world}" if world > 1 else "single"},
         "gpu_launches": args.steps,
+        "timing": spread,
         "cuda_graph": graphs is not None,
+        "graph_steps": copies if cycle is not None else 1,
         **({"graph_capture_error": capture_error} if capture_error else {}),
         "per_shape": per_shape,
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
@@ -1479,6 +1519,9 @@ def main():
     p.add_argument("--warmup", type=int, default=20)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--copies", type=int, default=4)
+    p.add_argument("--min-span-ms", type=float, default=200.0,
+                   help="the K-step timed region repeats until the repetitions span this long")
+    p.add_argument("--max-regions", type=int, default=5000)
     p.add_argument("--cpu-seconds", type=float, default=10.0)
     p.add_argument("--sections", default="encode,calibrated,batched,serving,archive_roi",
                    help="extra configs reported beside the headline (comma list, or none)")
