@@ -36,6 +36,7 @@ METRIC = "GPU decode GB/s (decoded uint16 pixels, 4096x4096 frame x 3 tile shape
 SHAPES = ((128, 32), (64, 64), (256, 16))
 W = H = 4096
 SEED = 2
+CYCLE = 20  # steps per replay of the headline's cycle graph (the driver's K)
 
 
 def measured_peaks():
@@ -238,12 +239,13 @@ def run_ours(args, rank, world, device, torch, dist):
         assert st == Status.success, st
 
     # CUDA graphs of the step: one per rotation slot (the decode of that slot's three archives),
-    # and one cycle graph holding the steps of every slot in order. Inside the cycle the decode
-    # kernels are programmatic dependents of one another, as consecutive executions in a stream
-    # are, so a step's launch overlaps the previous step's end; separate graph launches do not
-    # overlap. The executors validate pointers with cudaPointerGetAttributes on the host, which
+    # and one cycle graph holding CYCLE consecutive steps (the slots in rotation order). Inside
+    # the cycle the decode kernels are programmatic dependents of one another, as consecutive
+    # executions in a stream are, so a step's launch and parsed-payload staging overlap the
+    # previous step's end; separate graph launches do not overlap. The executors validate pointers with cudaPointerGetAttributes on the host, which
     # global-mode capture rejects, so capture is relaxed (the validation runs once, at capture).
     graphs, cycle, capture_error = [], None, None
+    cycle_steps = copies * max(1, CYCLE // copies)
     try:
         for slot in range(copies):
             g = torch.cuda.CUDAGraph()
@@ -252,8 +254,8 @@ def run_ours(args, rank, world, device, torch, dist):
             graphs.append(g)
         cycle = torch.cuda.CUDAGraph()
         with torch.cuda.graph(cycle, stream=stream, capture_error_mode="relaxed"):
-            for slot in range(copies):
-                enqueue(slot)
+            for k in range(cycle_steps):
+                enqueue(k % copies)
     except Exception as e:  # noqa: BLE001 - recorded in the JSON line, launches stay eager
         capture_error = str(e).splitlines()[0]
         print(f"graph capture failed, timing eager launches: {capture_error}", file=sys.stderr)
@@ -270,9 +272,9 @@ def run_ours(args, rank, world, device, torch, dist):
         """Steps first .. first + count - 1 (each one decode of its slot's three archives)."""
         i, end = first, first + count
         while i < end:
-            if cycle is not None and i % copies == 0 and end - i >= copies:
+            if cycle is not None and i % copies == 0 and end - i >= cycle_steps:
                 cycle.replay()
-                i += copies
+                i += cycle_steps
             else:
                 replay(i)
                 i += 1
@@ -380,7 +382,7 @@ def run_ours(args, rank, world, device, torch, dist):
         "gpu_launches": args.steps,
         "timing": spread,
         "cuda_graph": graphs is not None,
-        "graph_steps": copies if cycle is not None else 1,
+        "graph_steps": cycle_steps if cycle is not None else 1,
         **({"graph_capture_error": capture_error} if capture_error else {}),
         "per_shape": per_shape,
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,

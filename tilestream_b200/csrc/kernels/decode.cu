@@ -1022,9 +1022,12 @@ __device__ __forceinline__ void decode_body(Source &source, const tsk_row_start 
     if (warp == CW) {
         // Producer warp: lane 0 issues everything. The next task record is loaded before
         // waiting for a free stage, so its latency overlaps the consumers' work. Task records
-        // are the plan's (or the server's) own tables, written before any launch, so the first
-        // one is read before waiting for the stream's previous grid; payloads, which that grid
-        // may have produced, are read after.
+        // are the plan's (or the server's) own tables, written before any launch, and so are
+        // parsed payloads: a parsed source must stay byte-identical to the one validated when
+        // the plan was prepared, for as long as the plan is used (docs/api.md, "Batch plans and
+        // ownership"). Both are therefore read without waiting for the stream's previous grid,
+        // so the first stages fill while that grid finishes. Encoder output may be that grid's
+        // product: the first trusted task waits for it (griddep_wait) before it is staged.
         if (lane != 0) {
             return;
         }
@@ -1032,7 +1035,7 @@ __device__ __forceinline__ void decode_body(Source &source, const tsk_row_start 
         if (mine != 0) {
             t = source.task(blockIdx.x);
         }
-        griddep_wait();
+        bool waited = false;
         for (uint32_t i = 0; i < mine; ++i) {
             const uint32_t s = i % Stages;
             tsk_decode_task next{};
@@ -1045,6 +1048,10 @@ __device__ __forceinline__ void decode_body(Source &source, const tsk_row_start 
                 if (!freed) {
                     return; // consumers stopped; they have reported the timeout
                 }
+            }
+            if (!waited && (t.flags & TSK_TRUSTED)) {
+                griddep_wait();
+                waited = true;
             }
             stage_task(sh, s, t, source, rowtab);
             t = next;
@@ -1113,23 +1120,25 @@ __device__ __forceinline__ void decode_body_self(Source &source, const tsk_row_s
             named_sync(1 + group, RW * 32);
         }
     };
-    // Task records are the plan's (or the server's) own tables, written before any launch, so
-    // they are read before waiting for the stream's previous grid; payloads, outputs and
-    // results are touched after.
+    // Task records and parsed payloads are staged before waiting for the stream's previous
+    // grid (see decode_body); encoder output, outputs and results are touched after it.
     tsk_decode_task next{};
     if (lead && count > 0) {
         next = source.task(queue_index(0));
     }
-    griddep_wait();
     if (lead) {
         for (uint32_t k = 0; k < 2 && k < count; ++k) {
             const tsk_decode_task t = next;
             if (k + 1 < count) {
                 next = source.task(queue_index(k + 1));
             }
+            if (t.flags & TSK_TRUSTED) {
+                griddep_wait();
+            }
             stage_task(sh, 2 * group + k, t, source, rowtab);
         }
     }
+    griddep_wait();
     for (uint32_t k = 0; k < count; ++k) {
         const uint32_t s = 2 * group + (k & 1u);
         if (!mbar_wait(&sh.full[s], (k >> 1) & 1u)) {
@@ -1370,8 +1379,8 @@ extern "C" int tsk_decode_prepare(tsk_decode_config *config, uint32_t ntasks, in
 }
 
 // Launched as a programmatic dependent of the stream's previous grid: this grid's CTAs may
-// start (barrier set-up, first task record) while that grid finishes, and wait for it before
-// touching payloads, outputs or results (griddep_wait in decode_body).
+// start (barrier set-up, task records, parsed payloads) while that grid finishes, and wait for
+// it before reading encoder output or touching outputs and results (decode_body).
 extern "C" int tsk_decode_launch(const tsk_decode_task *tasks, uint32_t ntasks,
                                  const tsk_decode_image *images, const tsk_row_start *rows,
                                  tsk_result *results, tsk_decode_config config,
