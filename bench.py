@@ -239,12 +239,13 @@ def run_ours(args, rank, world, device, torch, dist):
         assert st == Status.success, st
 
     # CUDA graphs of the step: one per rotation slot (the decode of that slot's three archives),
-    # and one cycle graph holding CYCLE consecutive steps (the slots in rotation order). Inside
+    # and cycle graphs holding CYCLE consecutive steps (the slots in rotation order, one graph per
+    # starting slot). Inside
     # the cycle the decode kernels are programmatic dependents of one another, as consecutive
     # executions in a stream are, so a step's launch and parsed-payload staging overlap the
     # previous step's end; separate graph launches do not overlap. The executors validate pointers with cudaPointerGetAttributes on the host, which
     # global-mode capture rejects, so capture is relaxed (the validation runs once, at capture).
-    graphs, cycle, capture_error = [], None, None
+    graphs, cycles, capture_error = [], None, None
     cycle_steps = copies * max(1, CYCLE // copies)
     try:
         for slot in range(copies):
@@ -252,14 +253,17 @@ def run_ours(args, rank, world, device, torch, dist):
             with torch.cuda.graph(g, stream=stream, capture_error_mode="relaxed"):
                 enqueue(slot)
             graphs.append(g)
-        cycle = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(cycle, stream=stream, capture_error_mode="relaxed"):
-            for k in range(cycle_steps):
-                enqueue(k % copies)
+        cycles = []
+        for start in range(copies):
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g, stream=stream, capture_error_mode="relaxed"):
+                for k in range(cycle_steps):
+                    enqueue((start + k) % copies)
+            cycles.append(g)
     except Exception as e:  # noqa: BLE001 - recorded in the JSON line, launches stay eager
         capture_error = str(e).splitlines()[0]
         print(f"graph capture failed, timing eager launches: {capture_error}", file=sys.stderr)
-        graphs, cycle = None, None
+        graphs, cycles = None, None
     torch.cuda.synchronize()
 
     def replay(i):
@@ -268,17 +272,19 @@ def run_ours(args, rank, world, device, torch, dist):
         else:
             enqueue(i % copies)
 
-    def run_steps(first, count):
-        """Steps first .. first + count - 1 (each one decode of its slot's three archives)."""
-        i, end = first, first + count
-        while i < end:
-            if cycle is not None and i % copies == 0 and end - i >= cycle_steps:
-                cycle.replay()
-                i += cycle_steps
-            else:
-                replay(i)
-                i += 1
-        return end
+    position = [0]  # the rotation continues across calls: consecutive steps use other slots
+
+    def run_steps(count):
+        """count steps: cycle graphs (the one starting at the current slot), then single steps."""
+        i = 0
+        while cycles is not None and count - i >= cycle_steps:
+            cycles[position[0] % copies].replay()
+            i += cycle_steps
+            position[0] += cycle_steps
+        while i < count:
+            replay(position[0])
+            i += 1
+            position[0] += 1
 
     # Correctness of the benchmarked outputs (one slot per shape).
     for s in shapes:
@@ -291,14 +297,14 @@ def run_ours(args, rank, world, device, torch, dist):
     r = results.cpu().numpy().view(np.uint64).reshape(3, 2)
     assert all(int(r[k, 0]) == 0 and int(r[k, 1]) == W * H * 2 for k in range(3)), r
 
-    step_index = run_steps(0, args.warmup)
+    run_steps(args.warmup)
     torch.cuda.synchronize()
     # The timed region is K steps. It is repeated back to back until the repetitions span at
     # least 0.2 s (so that clock samples cover it), each region bracketed by its own events;
     # the reported time is the median region, with the spread beside it.
     pilot0, pilot1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     pilot0.record(stream)
-    step_index = run_steps(step_index, args.steps)
+    run_steps(args.steps)
     pilot1.record(stream)
     torch.cuda.synchronize()
     pilot_ms = max(pilot0.elapsed_time(pilot1), 1e-3)
@@ -311,7 +317,7 @@ def run_ours(args, rank, world, device, torch, dist):
     with ClockSampler(device) as clocks:
         for e0, e1 in events:
             e0.record(stream)
-            step_index = run_steps(step_index, args.steps)
+            run_steps(args.steps)
             e1.record(stream)
         torch.cuda.synchronize()
     if world > 1:
@@ -382,7 +388,7 @@ def run_ours(args, rank, world, device, torch, dist):
         "gpu_launches": args.steps,
         "timing": spread,
         "cuda_graph": graphs is not None,
-        "graph_steps": cycle_steps if cycle is not None else 1,
+        "graph_steps": cycle_steps if cycles is not None else 1,
         **({"graph_capture_error": capture_error} if capture_error else {}),
         "per_shape": per_shape,
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,

@@ -1284,6 +1284,12 @@ Variant select(uint32_t paths, uint32_t shape) {
             return make<16384, 2, kU16 | kF32 | kPlain, 4, 16, 5>();
         case 3:
             return make<16384, 2, kU16 | kF32 | kPlain, 4, 8, 6>();
+        case 4: // warp pairs per tile, two stages per pair
+            return make<16384, 4, kU16 | kF32 | kPlain, 4, 16, 3, 1, 2>();
+        case 5: // shape 1 with the single-pass uint16 rows
+            return make<16384, 2, kU16 | kF32 | kPlain, 4, 16, 5, 1>();
+        case 6: // shape 2 with the single-pass uint16 rows
+            return make<16384, 3, kU16 | kF32 | kPlain, 4, 16, 4, 1>();
         default:
             return narrow ? make<16384, 3, kU16 | kF32 | kPlain, 4, 16, 4>()
                           : make<16384, 3, kU16 | kF32 | kPlain>();
