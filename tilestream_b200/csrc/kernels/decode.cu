@@ -295,7 +295,7 @@ __device__ __forceinline__ void store(const Ctx &x, uint8_t *line, const uint8_t
         if (Full || (whole && (reinterpret_cast<uintptr_t>(dst) & 15u) == 0)) {
 #pragma unroll
             for (uint32_t k = 0; k < G; k += 4) {
-                *reinterpret_cast<uint4 *>(dst + k) = make_uint4(v[k], v[k + 1], v[k + 2], v[k + 3]);
+                st_global_v4(dst + k, v[k], v[k + 1], v[k + 2], v[k + 3]);
             }
         } else {
 #pragma unroll
@@ -600,9 +600,118 @@ __device__ __forceinline__ void predict_rows_u16(const Ctx &x, const uint32_t *p
     }
 }
 
+// Predictive FP32 rows: the same single-pass structure as predict_rows_u16 with G columns per
+// lane (G * LW is the class width: 64, 128 or 256 FP32 words, so a row is one pass), residuals
+// undone with XOR. The running XOR and the scan's conditional XOR need no multiply: a lane
+// takes its left neighbour's total masked by an all-ones or zero gate.
+template <uint32_t CW, uint32_t G, uint32_t LW, bool Cal, bool Full, bool AllLive>
+__device__ __forceinline__ void predict_rows_f32(const Ctx &x, const uint32_t *payload,
+                                                 const uint16_t *rows) {
+    constexpr uint32_t kRowsPerWarp = 32 / LW;
+    constexpr uint32_t kStride = CW * kRowsPerWarp;
+    constexpr uint32_t H = G / 2;
+    constexpr uint32_t kSteps = LW == 1 ? 0 : LW == 2 ? 1 : LW == 4 ? 2 : LW == 8 ? 3 : LW == 16 ? 4 : 5;
+    // CW here: the warps that share the tile; warp: this warp's slot among them.
+    const uint32_t warp = CW == 1 ? 0u : x.slot, lane = threadIdx.x % 32;
+    const uint32_t sub = lane % LW;
+    const uint32_t c0 = sub * G;
+    const uint32_t w = x.w;
+    const Pipes pipes{x.one, x.top};
+    uint32_t gate[kSteps > 0 ? kSteps : 1];
+#pragma unroll
+    for (uint32_t j = 0; j < kSteps; ++j) {
+        gate[j] = sub >= (1u << j) ? 0xffffffffu : 0u;
+    }
+    auto prefetch_maps = [&](uint32_t row) {
+        if constexpr (Cal) {
+            if (row < x.row1 && c0 < x.col1 && c0 + G > x.col0) {
+                const uint64_t line = static_cast<uint64_t>(row - x.row0);
+                const uint32_t c = c0 > x.col0 ? c0 : x.col0;
+                const uint32_t e = (c0 + G < x.col1 ? c0 + G : x.col1) - 1;
+                if (x.omap) {
+                    const uint8_t *m = x.omap + line * x.opitch;
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(m + 4 * c));
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(m + 4 * e));
+                }
+                if (x.gmap) {
+                    const uint8_t *m = x.gmap + line * x.gpitch;
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(m + 4 * c));
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(m + 4 * e));
+                }
+            }
+        }
+    };
+    if constexpr (Cal) {
+        prefetch_maps(x.row0 + warp * kRowsPerWarp + lane / LW);
+    }
+    for (uint32_t base = x.row0 + warp * kRowsPerWarp; base < x.row1; base += kStride) {
+        const uint32_t r = base + lane / LW;
+        const bool live = AllLive || r < x.row1;
+        if constexpr (Cal) {
+            prefetch_maps(r + kStride);
+        }
+        const uint64_t line_off = static_cast<uint64_t>(live ? r - x.row0 : 0u);
+        const uint32_t *row = payload + (live ? rows[r] : 0u);
+        const uint32_t width_byte = row[1] & 0xffu;
+        const uint32_t b = width_byte < 32u ? width_byte : 32u;
+        const uint32_t carry = row[0];
+        uint32_t t[G];
+        if (Full || c0 < w) {
+            terms<G, true, !Full>(row + 2, c0, w, b, pipes, t);
+        } else {
+#pragma unroll
+            for (uint32_t k = 0; k < G; ++k) {
+                t[k] = 0;
+            }
+        }
+#pragma unroll
+        for (uint32_t k = 1; k < G; ++k) {
+            if (k != H) {
+                t[k] ^= t[k - 1];
+            }
+        }
+        const uint32_t total = t[H - 1] ^ t[G - 1];
+        uint32_t inclusive = total;
+#pragma unroll
+        for (uint32_t j = 0; j < kSteps; ++j) {
+            const uint32_t other = __shfl_up_sync(kFull, inclusive, 1u << j, LW);
+            inclusive ^= other & gate[j];
+        }
+        if (AllLive || live) {
+            const uint32_t before = carry ^ inclusive ^ total;
+            const uint32_t mid = before ^ t[H - 1];
+            uint32_t v[G];
+#pragma unroll
+            for (uint32_t k = 0; k < G; ++k) {
+                v[k] = (k < H ? before : mid) ^ t[k];
+            }
+            uint8_t *line = x.out + line_off * x.pitch;
+            const uint8_t *orow = nullptr, *grow = nullptr;
+            if constexpr (Cal) {
+                orow = x.omap ? x.omap + line_off * x.opitch : nullptr;
+                grow = x.gmap ? x.gmap + line_off * x.gpitch : nullptr;
+            }
+            store<G, true, Cal, Full>(x, line, orow, grow, c0, v);
+        }
+    }
+}
+
 template <uint32_t CW, uint32_t G, uint32_t LW, bool F32, bool Cal, uint32_t NR>
 __device__ __forceinline__ void decode_class(const Ctx &x, const uint32_t *payload,
                                              const uint16_t *rows, uint32_t mode) {
+    if constexpr (F32 && NR != 0) {
+        if (mode == TSK_PREDICT) {
+            constexpr uint32_t kRowsPerIteration = CW * (32 / LW);
+            if (x.full && (x.row1 - x.row0) % kRowsPerIteration == 0) {
+                predict_rows_f32<CW, G, LW, Cal, true, true>(x, payload, rows);
+            } else if (x.full) {
+                predict_rows_f32<CW, G, LW, Cal, true, false>(x, payload, rows);
+            } else {
+                predict_rows_f32<CW, G, LW, Cal, false, false>(x, payload, rows);
+            }
+            return;
+        }
+    }
     if constexpr (!F32 && NR != 0) {
         if (mode == TSK_PREDICT) {
             constexpr uint32_t kRowsPerIteration = NR * CW * (32 / LW);
@@ -637,6 +746,15 @@ __device__ __forceinline__ void decode_tile(const Ctx &x, const uint32_t *payloa
             decode_class<CW, G16, 128 / G16, false, Cal, NR>(x, payload, rows, mode);
         } else {
             decode_class<CW, G16, 64 / G16, false, Cal, NR>(x, payload, rows, mode);
+        }
+    } else if constexpr (NR != 0) {
+        // 16 FP32 words per lane: every class width is one pass.
+        if (x.w > 128) {
+            decode_class<CW, 16, 16, true, Cal, NR>(x, payload, rows, mode);
+        } else if (x.w > 64) {
+            decode_class<CW, 16, 8, true, Cal, NR>(x, payload, rows, mode);
+        } else {
+            decode_class<CW, 16, 4, true, Cal, NR>(x, payload, rows, mode);
         }
     } else {
         if (x.w > 64) {
@@ -1265,16 +1383,20 @@ Variant select(uint32_t paths, uint32_t shape) {
             }
         }
         if (c && !plain) {
+            if (shape >= 8) return make<8192, 4, kU16 | kCal, 4, 16, 4, 1>();
             return narrow ? make<8192, 4, kU16 | kCal, 4, 16, 4>() : make<8192, 4, kU16 | kCal>();
         }
+        if (shape >= 8) return make<8192, 4, kU16 | kPlain | kCal, 4, 16, 4, 1>();
         return make<8192, 4, kU16 | kPlain | kCal>();
     }
     if (!u16) {
         if (plain && !c) {
+            if (shape >= 8) return make<16384, 3, kF32 | kPlain, 4, 16, 4, 1>();
             return narrow ? make<16384, 3, kF32 | kPlain, 4, 16, 4>()
                           : make<16384, 3, kF32 | kPlain>();
         }
         if (c && !plain) {
+            if (shape >= 8) return make<16384, 3, kF32 | kCal, 4, 16, 4, 1>();
             return narrow ? make<16384, 3, kF32 | kCal, 4, 16, 4>() : make<16384, 3, kF32 | kCal>();
         }
     } else if (plain && !c) {
@@ -1295,6 +1417,7 @@ Variant select(uint32_t paths, uint32_t shape) {
                           : make<16384, 3, kU16 | kF32 | kPlain>();
         }
     }
+    if (shape >= 8) return make<16384, 3, kU16 | kF32 | kPlain | kCal, 4, 16, 4, 1>();
     return narrow ? make<16384, 3, kU16 | kF32 | kPlain | kCal, 4, 16, 4>()
                   : make<16384, 3, kU16 | kF32 | kPlain | kCal>();
 }
