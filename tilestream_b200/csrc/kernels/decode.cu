@@ -1412,6 +1412,8 @@ Variant select(uint32_t paths, uint32_t shape) {
             return make<16384, 2, kU16 | kF32 | kPlain, 4, 16, 5, 1>();
         case 6: // shape 2 with the single-pass uint16 rows
             return make<16384, 3, kU16 | kF32 | kPlain, 4, 16, 4, 1>();
+        case 7: // shape 5 with six CTAs per SM
+            return make<16384, 2, kU16 | kF32 | kPlain, 4, 16, 6, 1>();
         default:
             return narrow ? make<16384, 3, kU16 | kF32 | kPlain, 4, 16, 4>()
                           : make<16384, 3, kU16 | kF32 | kPlain>();
