@@ -471,12 +471,85 @@ def run_e2e(args, torch, stream, shapes, wsb, recs):
         assert torch.equal(pinned_out[k], s["copies"][last]["out"].cpu())
     h2d = sum(len(s["file"]) for s in shapes)
     d2h = n * W * H * 2
-    return {"value": round(n * W * H * 2 * steps / (ms / 1e3) / 1e9, 2), "unit": "GB/s",
+
+    # From the file: every step starts from each archive's .tsc bytes in pinned host memory and
+    # runs parse_metadata (the library's host parser) and prepare_batch (a new plan) for it on
+    # the host, then the same copies and decode. The host parses and prepares step i + 1 while
+    # the GPU copies and decodes step i; a plan is released once the decode that used it has
+    # completed (two steps later, the slot's reuse).
+    prep_streams = [torch.cuda.Stream() for _ in shapes]
+    held = [[None, None] for _ in shapes]
+    fcounter = [0]
+
+    def step_file():
+        i = fcounter[0]
+        fcounter[0] += 1
+        slot = i % 2
+        for k, s in enumerate(shapes):
+            c = s["copies"][slot]
+            if held[k][slot] is not None:
+                decoded[k][slot].synchronize()  # the decode that used this slot's plan is done
+                held[k][slot] = None
+            st, meta = api.parse_metadata(pinned_in[k].numpy(), size=len(s["file"]))
+            assert st == 0, st
+            src = api.CompressedInput()
+            src.bytes = api.ConstBytes(c["src"].data_ptr(), len(s["file"]))
+            src.metadata = meta.handle
+            item = api.BatchItem()
+            item.compressed_input = src
+            item.output = api.view(c["out"], 1, W, H, W * 2)
+            st, plan = cuda.prepare_batch(cuda.make_request(cuda.Operation.decompress, [item]),
+                                          None, prep_streams[k])
+            assert st == 0, st
+            held[k][slot] = (meta, plan)
+            h, st_k = h2d_streams[k], streams[k]
+            if i >= 2:
+                h.wait_event(decoded[k][slot])
+            with torch.cuda.stream(h):
+                c["src"][:len(s["file"])].copy_(pinned_in[k], non_blocking=True)
+            copied[k][slot].record(h)
+            st_k.wait_event(copied[k][slot])
+            ws = api.MutableBytes(spaces[k].data_ptr(), spaces[k].numel())
+            assert cuda.decompress_async(plan, ws, own[k], st_k) == 0
+            decoded[k][slot].record(st_k)
+            with torch.cuda.stream(st_k):
+                pinned_out[k].copy_(c["out"], non_blocking=True)
+
+    def timed_file(count):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for st in streams + h2d_streams:
+            st.wait_event(e0)
+        for _ in range(count):
+            step_file()
+        for st in streams + h2d_streams:
+            stream.wait_stream(st)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    timed_file(4)
+    file_ms = timed_file(steps)
+    torch.cuda.synchronize()
+    held.clear()
+    recs_host = results.cpu().numpy().view(np.uint64).reshape(-1, 2)
+    assert all(int(r[0]) == 0 and int(r[1]) == W * H * 2 for r in recs_host), recs_host
+    last = (fcounter[0] - 1) % 2
+    for k, s in enumerate(shapes):
+        assert torch.equal(pinned_out[k], s["copies"][last]["out"].cpu())
+    from_file = {"value": round(n * W * H * 2 * steps / (file_ms / 1e3) / 1e9, 2), "unit": "GB/s",
+                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "steps": steps,
+                 "ms_per_step": round(file_ms / steps, 4),
+                 "host_work": "parse_metadata + prepare_batch of every archive, every step"}
+    resident = {"value": round(n * W * H * 2 * steps / (ms / 1e3) / 1e9, 2), "unit": "GB/s",
             "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "steps": steps,
             "ms_per_step": round(ms / steps, 4), "streams": 2 * n,
             "buffers": "two device copies per archive, alternating",
             "copies_only_ms_per_step": round(link_ms / steps, 4),
             "link_frac": round(link_ms / ms, 4)}
+    # The headline e2e is the like-for-like one: the reference arm's cpu::decompress also parses
+    # every file on every decode.
+    return {**from_file, "resident_plans": resident}
 
 
 def best_ms(fn, reps: int = 10) -> float:
