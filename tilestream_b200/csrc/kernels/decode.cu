@@ -267,18 +267,23 @@ __device__ __forceinline__ void store(const Ctx &x, uint8_t *line, const uint8_t
                              (grow ? reinterpret_cast<uintptr_t>(gm) : 0)) & 15u) == 0;
         }
         if (vec) {
+            // Every map load of the group is issued before any store: the output might alias a
+            // map as far as the compiler knows, so a load after a store would wait for it.
+            float4 o[G / 4], g[G / 4];
 #pragma unroll
             for (uint32_t k = 0; k < G; k += 4) {
-                float4 o = make_float4(x.offset, x.offset, x.offset, x.offset);
-                float4 g = make_float4(x.gain, x.gain, x.gain, x.gain);
-                if (orow) o = __ldg(reinterpret_cast<const float4 *>(om + k));
-                if (grow) g = __ldg(reinterpret_cast<const float4 *>(gm + k));
-                float4 r;
-                r.x = cal(as_value<F32>(v[k]), o.x, g.x);
-                r.y = cal(as_value<F32>(v[k + 1]), o.y, g.y);
-                r.z = cal(as_value<F32>(v[k + 2]), o.z, g.z);
-                r.w = cal(as_value<F32>(v[k + 3]), o.w, g.w);
-                *reinterpret_cast<float4 *>(dst + k) = r;
+                o[k / 4] = make_float4(x.offset, x.offset, x.offset, x.offset);
+                g[k / 4] = make_float4(x.gain, x.gain, x.gain, x.gain);
+                if (orow) o[k / 4] = __ldg(reinterpret_cast<const float4 *>(om + k));
+                if (grow) g[k / 4] = __ldg(reinterpret_cast<const float4 *>(gm + k));
+            }
+#pragma unroll
+            for (uint32_t k = 0; k < G; k += 4) {
+                const float4 ok = o[k / 4], gk = g[k / 4];
+                st_global_v4(dst + k, __float_as_uint(cal(as_value<F32>(v[k]), ok.x, gk.x)),
+                             __float_as_uint(cal(as_value<F32>(v[k + 1]), ok.y, gk.y)),
+                             __float_as_uint(cal(as_value<F32>(v[k + 2]), ok.z, gk.z)),
+                             __float_as_uint(cal(as_value<F32>(v[k + 3]), ok.w, gk.w)));
             }
         } else {
 #pragma unroll
