@@ -11,6 +11,9 @@
 // arrive while batches are running start on a free stream as soon as pool memory allows, so
 // their work overlaps on the device (continuous batching).
 //
+// Requests can also be submitted while the server runs (start, submit, wait, release, stop):
+// the same loop then serves them from a thread of its own as they come.
+//
 // The serial mode is the one-request-at-a-time baseline through the reference API:
 // prepare_batch, then decode_roi_async or decode_calibrate_async, then a synchronize, per
 // request.
@@ -87,6 +90,28 @@ class Server {
                              ServeOutcome *outcomes, ServeStats &stats) noexcept;
     // The output pool (device memory).
     [[nodiscard]] MutableBytes pool() const noexcept;
+
+    // ---- request sessions: requests submitted while the server runs ----
+    // start() launches the serving loop on a thread of its own: from then on, requests
+    // submitted from any thread are admitted by output-pool memory, batched into launches and
+    // overlapped on the GPU exactly as in run(). A request's output stays in the pool until the
+    // caller releases it, so results can be read at leisure. At most `max_outstanding` requests
+    // (submitted and not yet released) at a time. run() is not available while started.
+    [[nodiscard]] Status start(std::uint32_t max_outstanding = 4096) noexcept;
+    // Queues a request (arrival_us is ignored: it arrives now). ticket identifies it. Refused
+    // requests (unknown archive, ROI outside it, output larger than the pool) return their
+    // status here and take no ticket; resource_limit when too many are outstanding.
+    [[nodiscard]] Status submit(const ServeRequest &request, std::uint64_t &ticket) noexcept;
+    // Waits at most timeout_us for the request to complete; done tells whether it has. When
+    // done, outcome holds its result, output place and latency (submit to completion).
+    [[nodiscard]] Status wait(std::uint64_t ticket, std::uint64_t timeout_us,
+                              ServeOutcome &outcome, bool &done) noexcept;
+    // Gives the request's output memory back to the pool; the ticket is then unknown.
+    // invalid_argument for an unknown ticket or one that has not completed.
+    [[nodiscard]] Status release(std::uint64_t ticket) noexcept;
+    // Serves what was submitted, then ends the loop (unreleased outputs stay readable until the
+    // server is destroyed or started again).
+    [[nodiscard]] Status stop() noexcept;
 
     struct Impl;
 

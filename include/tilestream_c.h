@@ -196,6 +196,15 @@ int ts_server_seal(ts_server *server);
 int ts_server_run(ts_server *server, const ts_serve_request *requests, uint64_t count,
                   ts_serve_outcome *outcomes, ts_serve_stats *stats);
 int ts_server_pool(const ts_server *server, ts_mutable_bytes *pool);
+/* Sessions (Server::start/submit/wait/release/stop): requests submitted from any thread while
+ * the serving loop runs on a thread of its own. submit, wait and release are thread-safe; wait
+ * returns 0 with *done = 0 when timeout_us passes first. */
+int ts_server_start(ts_server *server, uint32_t max_outstanding);
+int ts_server_submit(ts_server *server, const ts_serve_request *request, uint64_t *ticket);
+int ts_server_wait(ts_server *server, uint64_t ticket, uint64_t timeout_us,
+                   ts_serve_outcome *outcome, int *done);
+int ts_server_release(ts_server *server, uint64_t ticket);
+int ts_server_stop(ts_server *server);
 void ts_server_destroy(ts_server *server);
 
 /* ---- ROI staging from an archive outside the GPU (include/tilestream/staging.h) ------------

@@ -1,7 +1,10 @@
 """ROI serving over resident archives: every request's output, served in a mix of co-arriving
 requests with continuous batching, equals the oracle's crop (or calibrated crop) and the same
 request served alone; the one-request-at-a-time plan path agrees; a small output pool forces
-admission stalls without changing any result; refusals are per request."""
+admission stalls without changing any result; refusals are per request. Sessions: requests
+submitted by two producer threads while the server runs, waited for (bounded) and released by a
+consumer thread, equal the oracle and the same request served alone; releases admit stalled
+requests, and stop settles what cannot be placed."""
 import numpy as np
 import pytest
 
@@ -230,3 +233,125 @@ def test_host_validation(cuda_ready, oracle_lib, fx):
         Status.malformed_data
     with pytest.raises(RuntimeError):
         cuda.Server(max_batch=49)
+
+
+# ---- sessions: requests submitted while the server runs --------------------------------------
+
+def _submit_bounded(srv, r, seconds=20.0):
+    """Submits r, retrying while too many requests are outstanding (bounded)."""
+    import time
+    end = time.monotonic() + seconds
+    while True:
+        st, ticket = srv.submit(r)
+        if st != Status.resource_limit or time.monotonic() > end:
+            return st, ticket
+        time.sleep(0.001)
+
+
+def _session_output(srv, outcome, r):
+    sample = 4 if (r.calibrated or ARCHIVES[r.archive][0] == "f32") else 2
+    rows = read_device(srv.pool().data + outcome.output_offset,
+                       outcome.output_pitch * r.roi.height)
+    rows = rows.reshape(r.roi.height, outcome.output_pitch)
+    return np.ascontiguousarray(rows[:, :r.roi.width * sample])
+
+
+def test_session_two_producers_one_consumer(cuda_ready, oracle_lib, fx):
+    """Two producer threads submit interleaved halves of a request stream while one consumer
+    waits (bounded), checks each output against the oracle and releases it. The pool holds
+    four of the largest outputs, so admission also waits for releases. Afterwards the same
+    requests served alone (run) give the same bytes."""
+    import queue
+    import threading
+    reqs = stream_of(240, seed=5007)
+    biggest = max(pool_need([r]) for r in reqs)
+    srv = fx.server(pool_bytes=4 * biggest, max_batch=16, max_inflight=4)
+    assert srv.submit(reqs[0])[0] == Status.invalid_argument  # not started
+    assert srv.start(max_outstanding=32) == Status.success
+    assert srv.run(reqs)[0] == Status.invalid_argument  # run() is closed while started
+    handed = queue.Queue()
+    errors = []
+
+    def producer(part):
+        for i in range(part, len(reqs), 2):
+            st, ticket = _submit_bounded(srv, reqs[i])
+            if st != Status.success:
+                errors.append((i, st))
+                handed.put(None)
+                return
+            handed.put((i, ticket))
+
+    threads = [threading.Thread(target=producer, args=(p,)) for p in (0, 1)]
+    for t in threads:
+        t.start()
+    got, batches = {}, []
+    try:
+        for _ in range(len(reqs)):
+            item = handed.get(timeout=60)
+            assert item is not None, errors
+            i, ticket = item
+            st, done, oc = srv.wait(ticket, timeout_us=10_000_000)
+            assert st == Status.success and done, (i, st, done)
+            assert oc.result.status == 0 and oc.batch_size >= 1, i
+            want, _ = expected(oracle_lib, fx, reqs[i])
+            assert oc.result.bytes_written == want.size, i
+            out = _session_output(srv, oc, reqs[i])
+            assert same(out, want, reqs[i].calibrated != 0), i
+            got[i] = out
+            batches.append(oc.batch_size)
+            assert srv.release(ticket) == Status.success
+            assert srv.release(ticket) == Status.invalid_argument  # released already
+    finally:
+        for t in threads:
+            t.join(timeout=60)
+        assert srv.stop() == Status.success
+    assert not errors and len(got) == len(reqs)
+    assert max(batches) > 1  # requests from both producers shared launches
+    for i in range(0, len(reqs), 9):
+        one = (cuda.N.ServeRequest * 1)(reqs[i])
+        one[0].arrival_us = 0.0
+        st, oc, _ = srv.run(one)
+        assert st == Status.success and oc[0].batch_size == 1
+        assert same(_session_output(srv, oc[0], one[0]), got[i], one[0].calibrated != 0), i
+
+
+def test_session_release_admits_and_stop_settles(cuda_ready, oracle_lib, fx):
+    """A pool with room for one output: the second request waits for the first's release (a
+    bounded wait reports not done meanwhile); at stop, a request that cannot be placed while
+    an output is held completes with resource_limit."""
+    r = stream_of(1, seed=5008)[0]
+    r.archive, r.roi, r.calibrated = 0, api.Roi(0, 0, 1000, 700), 0
+    size = pool_need([r])
+    srv = fx.server(pool_bytes=size)
+    assert srv.start(max_outstanding=2) == Status.success
+    st, a = srv.submit(r)
+    assert st == Status.success
+    st, b = srv.submit(r)
+    assert st == Status.success
+    assert srv.submit(r)[0] == Status.resource_limit  # two outstanding
+    st, done, oa = srv.wait(a, timeout_us=10_000_000)
+    assert st == Status.success and done and oa.result.status == 0
+    want, _ = expected(oracle_lib, fx, r)
+    assert np.array_equal(_session_output(srv, oa, r), want)
+    st, done, _ = srv.wait(b, timeout_us=200_000)
+    assert st == Status.success and not done  # held: a's output occupies the pool
+    assert srv.release(b) == Status.invalid_argument  # not complete
+    assert srv.release(a) == Status.success
+    st, done, ob = srv.wait(b, timeout_us=10_000_000)
+    assert st == Status.success and done and ob.result.status == 0
+    assert np.array_equal(_session_output(srv, ob, r), want)
+    # b's output is held: c cannot be placed, and stop settles it.
+    st, c = srv.submit(r)
+    assert st == Status.success
+    assert srv.stop() == Status.success
+    st, done, oc = srv.wait(c, timeout_us=0)
+    assert st == Status.success and done
+    assert oc.result.status == int(Status.resource_limit) and oc.result.bytes_written == 0
+    assert srv.wait(12345, timeout_us=0)[0] == Status.invalid_argument  # unknown ticket
+    assert srv.stop() == Status.invalid_argument  # not started
+    # Started again: a fresh session over the same archives.
+    assert srv.start() == Status.success
+    st, d = srv.submit(r)
+    st, done, od = srv.wait(d, timeout_us=10_000_000)
+    assert st == Status.success and done and od.result.status == 0 and od.output_offset == 0
+    assert srv.stop() == Status.success

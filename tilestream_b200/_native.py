@@ -193,6 +193,11 @@ _SIGNATURES = {
     "ts_server_run": (C.c_int, [vp, C.POINTER(ServeRequest), u64, C.POINTER(ServeOutcome),
                                 C.POINTER(ServeStats)]),
     "ts_server_pool": (C.c_int, [vp, C.POINTER(MutableBytes)]),
+    "ts_server_start": (C.c_int, [vp, u32]),
+    "ts_server_submit": (C.c_int, [vp, C.POINTER(ServeRequest), C.POINTER(u64)]),
+    "ts_server_wait": (C.c_int, [vp, u64, u64, C.POINTER(ServeOutcome), C.POINTER(C.c_int)]),
+    "ts_server_release": (C.c_int, [vp, u64]),
+    "ts_server_stop": (C.c_int, [vp]),
     "ts_server_destroy": (None, [vp]),
     "ts_roi_staging_size": (C.c_int, [vp, Roi, C.POINTER(RoiStaging)]),
     "ts_stage_roi_tiles": (C.c_int, [vp, Roi, ConstBytes, MutableBytes, C.POINTER(TileMapping),

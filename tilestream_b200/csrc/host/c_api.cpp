@@ -455,6 +455,48 @@ extern "C" int ts_server_pool(const ts_server *server, ts_mutable_bytes *pool) {
     return 0;
 }
 
+extern "C" int ts_server_start(ts_server *server, uint32_t max_outstanding) {
+    if (server == nullptr || !server->server) {
+        return code(ts::Status::invalid_argument);
+    }
+    return code(server->server->start(max_outstanding));
+}
+
+extern "C" int ts_server_submit(ts_server *server, const ts_serve_request *request,
+                                uint64_t *ticket) {
+    if (server == nullptr || !server->server || request == nullptr || ticket == nullptr) {
+        return code(ts::Status::invalid_argument);
+    }
+    return code(server->server->submit(*reinterpret_cast<const ts::cuda::ServeRequest *>(request),
+                                       *ticket));
+}
+
+extern "C" int ts_server_wait(ts_server *server, uint64_t ticket, uint64_t timeout_us,
+                              ts_serve_outcome *outcome, int *done) {
+    if (server == nullptr || !server->server || outcome == nullptr || done == nullptr) {
+        return code(ts::Status::invalid_argument);
+    }
+    bool finished = false;
+    const ts::Status st = server->server->wait(
+        ticket, timeout_us, *reinterpret_cast<ts::cuda::ServeOutcome *>(outcome), finished);
+    *done = finished ? 1 : 0;
+    return code(st);
+}
+
+extern "C" int ts_server_release(ts_server *server, uint64_t ticket) {
+    if (server == nullptr || !server->server) {
+        return code(ts::Status::invalid_argument);
+    }
+    return code(server->server->release(ticket));
+}
+
+extern "C" int ts_server_stop(ts_server *server) {
+    if (server == nullptr || !server->server) {
+        return code(ts::Status::invalid_argument);
+    }
+    return code(server->server->stop());
+}
+
 extern "C" void ts_server_destroy(ts_server *server) {
     delete server;
 }

@@ -7,7 +7,9 @@
 // the same clip that the planner applies per tile (reference plan.cpp:281-349 selects the
 // intersecting tiles, tests/cuda_decoder_test.cpp:19-31).
 //
-// The loop runs on the calling thread. On each pass it:
+// run() drives the loop on the calling thread over a known request stream; start() drives the
+// same loop on a thread of its own over requests that callers submit while it runs. On each
+// pass the loop:
 //   1. polls the in-flight launches' events and records the completion time of their requests;
 //   2. frees the output memory of finished requests (unless outputs are retained);
 //   3. admits the requests that have arrived, in arrival order, while the output pool has room;
@@ -21,9 +23,13 @@
 
 #include <algorithm>
 #include <chrono>
+#include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <mutex>
 #include <new>
+#include <thread>
+#include <unordered_map>
 #include <vector>
 
 namespace tilestream::cuda {
@@ -110,6 +116,55 @@ struct Slot {
     std::uint64_t r0 = 0, r1 = 0; // requests [r0, r1)
 };
 
+// One request of a session, from submit() to release().
+struct Ticket {
+    ServeRequest request;
+    std::uint64_t bytes = 0, tiles = 0;
+    std::uint64_t seq = 0;  // its block in the ring, when placed
+    bool placed = false;    // output memory allocated
+    bool done = false;      // outcome final
+    Clock::time_point submitted;
+    ServeOutcome outcome;
+};
+
+// The state shared by the session thread and the callers, guarded by `mu`.
+struct Session {
+    std::mutex mu;
+    std::condition_variable completed; // callers waiting for a request
+    std::condition_variable wake;      // the session thread, idle
+    std::thread worker;
+    std::unordered_map<std::uint64_t, Ticket> tickets;
+    std::deque<std::uint64_t> queue; // submitted, not yet admitted, in submission order
+    std::vector<std::vector<std::uint64_t>> launched; // per slot: its batch's tickets
+    std::unique_ptr<Ring> ring;
+    std::uint64_t next_ticket = 1;
+    std::uint32_t max_outstanding = 0;
+    bool running = false, stopping = false;
+    Status failure = Status::success;
+    tsk_result *device_records = nullptr; // per slot: max_batch records
+    tsk_result *host_records = nullptr;   // pinned copies of them
+};
+
+// The launch record of request q, output at `out` with rows `pitch` bytes apart.
+void fill_record(tsk_serve_request &rec, const ServeRequest &q, const ArchiveEntry &a,
+                 std::uint64_t out, std::uint64_t pitch) {
+    const TileShape tile = a.metadata->tile;
+    rec.out = out;
+    rec.out_pitch = pitch;
+    rec.archive = q.archive;
+    rec.x = q.roi.x;
+    rec.y = q.roi.y;
+    rec.width = q.roi.width;
+    rec.height = q.roi.height;
+    rec.left = q.roi.x / tile.width;
+    rec.top = q.roi.y / tile.height;
+    rec.across = static_cast<std::uint32_t>(
+        (std::uint64_t{q.roi.x} + q.roi.width - 1) / tile.width - rec.left + 1);
+    rec.flags = q.calibrated != 0 ? TSK_CALIBRATED : 0;
+    rec.offset = q.offset;
+    rec.gain = q.gain;
+}
+
 } // namespace
 
 struct Server::Impl {
@@ -126,8 +181,12 @@ struct Server::Impl {
     const tsk_row_start *dev_rows = nullptr;
     std::uint32_t grid = 0;
     std::vector<Slot> slots;
+    Session session;
 
     ~Impl() {
+        end_session();
+        if (session.device_records != nullptr) cudaFree(session.device_records);
+        if (session.host_records != nullptr) cudaFreeHost(session.host_records);
         for (Slot &s : slots) {
             if (s.done != nullptr) cudaEventDestroy(s.done);
             if (s.stream != nullptr) cudaStreamDestroy(s.stream);
@@ -140,6 +199,16 @@ struct Server::Impl {
                        ServeStats &stats);
     Status run_serial(const ServeRequest *requests, std::uint64_t count, ServeOutcome *outcomes,
                       ServeStats &stats);
+    void session_loop();
+    void settle_queued(Status status);
+    void end_session() {
+        {
+            std::lock_guard<std::mutex> lock(session.mu);
+            session.stopping = true;
+        }
+        session.wake.notify_all();
+        if (session.worker.joinable()) session.worker.join();
+    }
 };
 
 Server::Server(std::unique_ptr<Impl> impl) noexcept : impl_(std::move(impl)) {}
@@ -371,6 +440,12 @@ Status Server::run(const ServeRequest *requests, std::uint64_t count, ServeOutco
     if (!s.sealed || (count != 0 && (requests == nullptr || outcomes == nullptr))) {
         return Status::invalid_argument;
     }
+    {
+        std::lock_guard<std::mutex> lock(s.session.mu);
+        if (s.session.running) {
+            return Status::invalid_argument;
+        }
+    }
     for (std::uint64_t i = 1; i < count; ++i) {
         if (!(requests[i].arrival_us >= requests[i - 1].arrival_us)) {
             return Status::invalid_argument;
@@ -496,23 +571,10 @@ Status Server::Impl::run_batched(const ServeRequest *requests, std::uint64_t cou
             }
             if (bytes[next] != 0) {
                 const ServeRequest &q = requests[next];
-                const ArchiveEntry &a = archives[q.archive];
-                const TileShape tile = a.metadata->tile;
                 tsk_serve_request &rec = batch.requests[n];
-                rec.out = reinterpret_cast<std::uint64_t>(pool) + offset;
-                rec.out_pitch = outcomes[next].output_pitch;
-                rec.archive = q.archive;
-                rec.x = q.roi.x;
-                rec.y = q.roi.y;
-                rec.width = q.roi.width;
-                rec.height = q.roi.height;
-                rec.left = q.roi.x / tile.width;
-                rec.top = q.roi.y / tile.height;
-                rec.across = static_cast<std::uint32_t>(
-                    (std::uint64_t{q.roi.x} + q.roi.width - 1) / tile.width - rec.left + 1);
-                rec.flags = q.calibrated != 0 ? TSK_CALIBRATED : 0;
-                rec.offset = q.offset;
-                rec.gain = q.gain;
+                fill_record(rec, q, archives[q.archive],
+                            reinterpret_cast<std::uint64_t>(pool) + offset,
+                            outcomes[next].output_pitch);
                 ntasks += tiles[next];
                 rec.task_end = static_cast<std::uint32_t>(ntasks);
                 outcomes[next].output_offset = offset;
@@ -716,6 +778,294 @@ Status Server::Impl::run_serial(const ServeRequest *requests, std::uint64_t coun
     stats.mean_batch = stats.batches != 0 ? 1.0 : 0.0;
     summarize(count, outcomes, micros(t0, last), stats);
     return Status::success;
+}
+
+// ---- sessions ---------------------------------------------------------------------------
+
+Status Server::start(std::uint32_t max_outstanding) noexcept {
+    Impl &s = *impl_;
+    Session &S = s.session;
+    std::lock_guard<std::mutex> lock(S.mu);
+    if (!s.sealed || S.running || s.options.serial != 0 || max_outstanding == 0) {
+        return Status::invalid_argument;
+    }
+    if (S.worker.joinable()) {
+        S.worker.join(); // a loop that ended on a failure
+    }
+    const std::uint64_t records = std::uint64_t{s.options.max_inflight} * s.options.max_batch;
+    if (S.device_records == nullptr) {
+        if (cudaMalloc(reinterpret_cast<void **>(&S.device_records),
+                       records * sizeof(tsk_result)) != cudaSuccess) {
+            S.device_records = nullptr;
+            cudaGetLastError();
+            return Status::resource_limit;
+        }
+        if (cudaMallocHost(reinterpret_cast<void **>(&S.host_records),
+                           records * sizeof(tsk_result)) != cudaSuccess) {
+            S.host_records = nullptr;
+            cudaGetLastError();
+            return Status::resource_limit;
+        }
+    }
+    try {
+        S.ring = std::make_unique<Ring>(s.options.output_pool_bytes);
+        S.tickets.clear();
+        S.queue.clear();
+        S.launched.assign(s.slots.size(), {});
+        for (std::vector<std::uint64_t> &ids : S.launched) {
+            ids.reserve(s.options.max_batch); // no allocation on the session thread
+        }
+        S.max_outstanding = max_outstanding;
+        S.failure = Status::success;
+        S.stopping = false;
+        S.running = true;
+        S.worker = std::thread([&s] { s.session_loop(); });
+    } catch (...) {
+        S.running = false;
+        return Status::resource_limit;
+    }
+    return Status::success;
+}
+
+Status Server::submit(const ServeRequest &request, std::uint64_t &ticket) noexcept {
+    Impl &s = *impl_;
+    Session &S = s.session;
+    Ticket t;
+    t.request = request;
+    const Status st = check_request(request, s.archives, s.options.output_pool_bytes,
+                                    t.outcome.output_pitch, t.bytes, t.tiles);
+    if (st != Status::success) {
+        return st;
+    }
+    {
+        std::lock_guard<std::mutex> lock(S.mu);
+        if (!S.running || S.stopping) {
+            return Status::invalid_argument;
+        }
+        if (S.failure != Status::success) {
+            return S.failure;
+        }
+        if (S.tickets.size() >= S.max_outstanding) {
+            return Status::resource_limit;
+        }
+        t.submitted = Clock::now();
+        try {
+            const std::uint64_t id = S.next_ticket;
+            S.tickets.emplace(id, t);
+            S.queue.push_back(id);
+            ++S.next_ticket;
+            ticket = id;
+        } catch (const std::bad_alloc &) {
+            S.tickets.erase(S.next_ticket);
+            return Status::resource_limit;
+        }
+    }
+    S.wake.notify_one();
+    return Status::success;
+}
+
+Status Server::wait(std::uint64_t ticket, std::uint64_t timeout_us, ServeOutcome &outcome,
+                    bool &done) noexcept {
+    Session &S = impl_->session;
+    done = false;
+    std::unique_lock<std::mutex> lock(S.mu);
+    // Bounded at about 12 days so that the deadline cannot overflow.
+    const auto limit = std::chrono::microseconds(std::min<std::uint64_t>(timeout_us, 1ull << 40));
+    const bool settled = S.completed.wait_for(lock, limit, [&] {
+        const auto it = S.tickets.find(ticket);
+        return it == S.tickets.end() || it->second.done || S.failure != Status::success;
+    });
+    const auto it = S.tickets.find(ticket);
+    if (it == S.tickets.end()) {
+        return Status::invalid_argument;
+    }
+    if (it->second.done) {
+        outcome = it->second.outcome;
+        done = true;
+        return Status::success;
+    }
+    return settled ? S.failure : Status::success;
+}
+
+Status Server::release(std::uint64_t ticket) noexcept {
+    Session &S = impl_->session;
+    {
+        std::lock_guard<std::mutex> lock(S.mu);
+        const auto it = S.tickets.find(ticket);
+        if (it == S.tickets.end() || !it->second.done) {
+            return Status::invalid_argument;
+        }
+        if (it->second.placed) {
+            S.ring->release(it->second.seq);
+        }
+        S.tickets.erase(it);
+    }
+    S.wake.notify_one(); // output memory came back: a stalled request may fit now
+    return Status::success;
+}
+
+Status Server::stop() noexcept {
+    Impl &s = *impl_;
+    Session &S = s.session;
+    {
+        std::lock_guard<std::mutex> lock(S.mu);
+        if (!S.running) {
+            return Status::invalid_argument;
+        }
+    }
+    s.end_session();
+    std::lock_guard<std::mutex> lock(S.mu);
+    S.running = false;
+    S.stopping = false;
+    return S.failure;
+}
+
+// Gives every queued request the final status `status` (no output). Called with the lock held.
+void Server::Impl::settle_queued(Status status) {
+    for (const std::uint64_t id : session.queue) {
+        Ticket &t = session.tickets.at(id);
+        t.outcome.result.status = status;
+        t.outcome.result.bytes_written = 0;
+        t.done = true;
+    }
+    session.queue.clear();
+}
+
+void Server::Impl::session_loop() {
+    Session &S = session;
+    const bool device_ok = cudaSetDevice(device) == cudaSuccess;
+    std::unique_lock<std::mutex> lock(S.mu);
+    if (!device_ok) {
+        S.failure = Status::cuda_error;
+    }
+    tsk_serve_batch batch;
+    const std::uint32_t limit = options.max_batch;
+    while (S.failure == Status::success) {
+        // 1. Completions: the batch's records were copied to pinned memory in stream order.
+        bool busy = false, finished = false;
+        for (std::size_t k = 0; k < slots.size(); ++k) {
+            Slot &slot = slots[k];
+            if (!slot.busy) continue;
+            const cudaError_t q = cudaEventQuery(slot.done);
+            if (q == cudaErrorNotReady) {
+                busy = true;
+                continue;
+            }
+            if (q != cudaSuccess) {
+                S.failure = detail::cuda_failure("serving batch", q);
+                break;
+            }
+            const Clock::time_point now = Clock::now();
+            const tsk_result *rec = S.host_records + k * limit;
+            const std::vector<std::uint64_t> &ids = S.launched[k];
+            for (std::size_t j = 0; j < ids.size(); ++j) {
+                Ticket &t = S.tickets.at(ids[j]);
+                t.outcome.result.status = static_cast<Status>(rec[j].status);
+                t.outcome.result.bytes_written = rec[j].bytes_written;
+                t.outcome.latency_us = micros(t.submitted, now);
+                t.done = true;
+            }
+            S.launched[k].clear();
+            slot.busy = false;
+            finished = true;
+        }
+        if (finished) {
+            S.completed.notify_all();
+        }
+        if (S.failure != Status::success) break;
+        // 2. Admission, in submission order, while the pool has room; then one launch.
+        std::size_t free_slot = slots.size();
+        for (std::size_t k = 0; k < slots.size(); ++k) {
+            if (!slots[k].busy) {
+                free_slot = k;
+                break;
+            }
+        }
+        bool stalled = false;
+        if (free_slot < slots.size() && !S.queue.empty()) {
+            std::uint32_t n = 0;
+            std::uint64_t ntasks = 0;
+            std::vector<std::uint64_t> &ids = S.launched[free_slot];
+            while (!S.queue.empty() && n < limit) {
+                Ticket &t = S.tickets.at(S.queue.front());
+                if (ntasks + t.tiles > options.max_batch_tiles && n != 0) break;
+                std::uint64_t offset = 0;
+                if (!S.ring->alloc(t.bytes, offset, t.seq)) {
+                    stalled = true;
+                    break;
+                }
+                t.placed = true;
+                t.outcome.output_offset = offset;
+                fill_record(batch.requests[n], t.request, archives[t.request.archive],
+                            reinterpret_cast<std::uint64_t>(pool) + offset,
+                            t.outcome.output_pitch);
+                ntasks += t.tiles;
+                batch.requests[n].task_end = static_cast<std::uint32_t>(ntasks);
+                ids.push_back(S.queue.front());
+                S.queue.pop_front();
+                ++n;
+            }
+            if (n != 0) {
+                batch.count = n;
+                batch.ntasks = static_cast<std::uint32_t>(ntasks);
+                Slot &slot = slots[free_slot];
+                tsk_result *dev = S.device_records + free_slot * limit;
+                const int e = tsk_serve_launch(&batch, dev_archives, dev_rows, dev, grid,
+                                               all_u16 ? 1 : 0, slot.stream);
+                if (e != 0 ||
+                    cudaMemcpyAsync(S.host_records + free_slot * limit, dev,
+                                    n * sizeof(tsk_result), cudaMemcpyDeviceToHost,
+                                    slot.stream) != cudaSuccess ||
+                    cudaEventRecord(slot.done, slot.stream) != cudaSuccess) {
+                    S.failure = detail::cuda_failure("serving launch", static_cast<cudaError_t>(e));
+                    break;
+                }
+                const Clock::time_point at = Clock::now();
+                for (const std::uint64_t id : ids) {
+                    Ticket &t = S.tickets.at(id);
+                    t.outcome.queued_us = micros(t.submitted, at);
+                    t.outcome.batch_size = n;
+                }
+                slot.busy = true;
+                busy = true;
+            }
+        }
+        if (S.stopping && !busy && (S.queue.empty() || stalled)) {
+            // Requests that cannot fit while the outputs before them are held stay unserved.
+            settle_queued(Status::resource_limit);
+            S.completed.notify_all();
+            break;
+        }
+        if (busy) {
+            // Poll the in-flight launches without holding the lock.
+            lock.unlock();
+            std::this_thread::yield();
+            lock.lock();
+        } else if (S.queue.empty() || stalled) {
+            // Idle until a submit, a release or stop (or, at the latest, a millisecond).
+            S.wake.wait_for(lock, std::chrono::milliseconds(1));
+        }
+    }
+    if (S.failure != Status::success) {
+        lock.unlock();
+        for (Slot &slot : slots) {
+            if (slot.busy) {
+                cudaEventSynchronize(slot.done);
+                slot.busy = false;
+            }
+        }
+        lock.lock();
+        for (std::vector<std::uint64_t> &ids : S.launched) {
+            for (const std::uint64_t id : ids) {
+                Ticket &t = S.tickets.at(id);
+                t.outcome.result.status = S.failure;
+                t.done = true;
+            }
+            ids.clear();
+        }
+        settle_queued(S.failure);
+        S.completed.notify_all();
+    }
 }
 
 } // namespace tilestream::cuda

@@ -230,6 +230,30 @@ class Server:
         st = N.lib().ts_server_run(self.handle, arr, count, outcomes, C.byref(stats))
         return Status(st), outcomes, stats
 
+    # Sessions: requests submitted while the serving loop runs on a thread of its own. The
+    # native calls release the GIL, so producers and consumers may be Python threads.
+    def start(self, max_outstanding=4096) -> Status:
+        return Status(N.lib().ts_server_start(self.handle, max_outstanding))
+
+    def submit(self, request) -> tuple[Status, int]:
+        """request: an N.ServeRequest (arrival_us ignored). Returns (Status, ticket)."""
+        t = C.c_uint64(0)
+        st = N.lib().ts_server_submit(self.handle, C.byref(request), C.byref(t))
+        return Status(st), t.value
+
+    def wait(self, ticket, timeout_us=1_000_000):
+        """(Status, done, ServeOutcome): done is False when timeout_us passed first."""
+        out = N.ServeOutcome()
+        done = C.c_int(0)
+        st = N.lib().ts_server_wait(self.handle, ticket, timeout_us, C.byref(out), C.byref(done))
+        return Status(st), bool(done.value), out
+
+    def release(self, ticket) -> Status:
+        return Status(N.lib().ts_server_release(self.handle, ticket))
+
+    def stop(self) -> Status:
+        return Status(N.lib().ts_server_stop(self.handle))
+
     def __del__(self, _lib=N.lib):
         # _lib is bound at definition: module globals may already be gone at interpreter exit.
         if getattr(self, "handle", None):
