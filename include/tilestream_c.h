@@ -243,6 +243,30 @@ int ts_compress_noalloc(ts_const_image_view input, ts_tile_shape tile, ts_mutabl
                         ts_device_result *result, void *stream);
 uint64_t ts_compress_noalloc_max_tiles(void);
 
+/* ---- TIFF import and export (include/tilestream/tiff.h; reference tiff.h:10-37) --------- */
+typedef struct {
+    uint32_t max_width, max_height;
+    uint64_t max_decoded_bytes;
+} ts_tiff_read_limits; /* TiffReadLimits */
+typedef struct {
+    uint32_t bigtiff;              /* nonzero: BigTIFF */
+    uint32_t compression;          /* 0 none, 1 deflate */
+    uint32_t horizontal_predictor; /* nonzero: predictor 2 (uint16 + deflate only) */
+    uint32_t tile_width, tile_height, deflate_level;
+} ts_tiff_write_options; /* TiffWriteOptions, field by field */
+/* An owned tilestream::io::TiffImage. */
+typedef struct ts_tiff_image ts_tiff_image;
+
+/* io::read_tiff (tiff.h:34-35). limits NULL: none. *image is replaced only on success. */
+int ts_read_tiff(const char *path, const ts_tiff_read_limits *limits, ts_tiff_image **image);
+/* The image's spec, row pitch and packed pixels (host memory owned by the image). */
+int ts_tiff_image_pixels(const ts_tiff_image *image, ts_image_spec *spec, uint64_t *pitch_bytes,
+                         const void **pixels, uint64_t *bytes);
+void ts_tiff_image_destroy(ts_tiff_image *image);
+/* io::write_tiff (tiff.h:36-37); image is host memory. options NULL: defaults. */
+int ts_write_tiff(const char *path, ts_const_image_view image,
+                  const ts_tiff_write_options *options);
+
 /* ---- plan inspection (extension, no reference counterpart) ---------------------------------
  * For validation tooling. Runs the host half of ts_prepare_batch for a decode request
  * (decompress, decode_roi or decode_calibrate): every argument, metadata, ROI, capacity and

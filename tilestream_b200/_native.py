@@ -73,6 +73,28 @@ class ParseLimits(C.Structure):
     _fields_ = [("file_bytes", u64), ("tile_count", u64), ("metadata_bytes", u64)]
 
 
+class TiffReadLimits(C.Structure):
+    _fields_ = [("max_width", u32), ("max_height", u32), ("max_decoded_bytes", u64)]
+
+    def __init__(self, *args, **kw):
+        super().__init__(*args, **kw)
+        if not args and not kw:
+            self.max_width = self.max_height = 0xFFFFFFFF
+            self.max_decoded_bytes = (1 << 63) - 1
+
+
+class TiffWriteOptions(C.Structure):
+    _fields_ = [("bigtiff", u32), ("compression", u32), ("horizontal_predictor", u32),
+                ("tile_width", u32), ("tile_height", u32), ("deflate_level", u32)]
+
+    def __init__(self, *args, **kw):
+        super().__init__(*args, **kw)
+        if not args:
+            for k, v in (("tile_width", 128), ("tile_height", 32), ("deflate_level", 6)):
+                if k not in kw:
+                    setattr(self, k, v)
+
+
 class WorkspaceSpec(C.Structure):
     _fields_ = [("image_count", u64), ("tile_count", u64), ("tile", TileShape),
                 ("scan_temp_bytes", u64)]
@@ -202,6 +224,11 @@ _SIGNATURES = {
     "ts_roi_staging_size": (C.c_int, [vp, Roi, C.POINTER(RoiStaging)]),
     "ts_stage_roi_tiles": (C.c_int, [vp, Roi, ConstBytes, MutableBytes, C.POINTER(TileMapping),
                                      u64, vp, C.POINTER(RoiStaging)]),
+    "ts_read_tiff": (C.c_int, [C.c_char_p, C.POINTER(TiffReadLimits), C.POINTER(vp)]),
+    "ts_tiff_image_pixels": (C.c_int, [vp, C.POINTER(ImageSpec), C.POINTER(u64),
+                                       C.POINTER(vp), C.POINTER(u64)]),
+    "ts_tiff_image_destroy": (None, [vp]),
+    "ts_write_tiff": (C.c_int, [C.c_char_p, ConstImageView, C.POINTER(TiffWriteOptions)]),
     "ts_compress_noalloc": (C.c_int, [ConstImageView, TileShape, MutableBytes, vp, vp]),
     "ts_compress_noalloc_max_tiles": (u64, []),
     "ts_device_allocate": (C.c_int, [u64, vp, C.POINTER(vp)]),

@@ -8,6 +8,7 @@ from __future__ import annotations
 
 import ctypes as C
 import enum
+import os
 
 import numpy as np
 
@@ -15,7 +16,7 @@ from . import _native as N
 from ._native import (BatchItem, BatchRequest, Calibration, CompressedInput, ConstBytes,  # noqa
                       ConstImageView, DeviceResult, ImageSpec, ImageView, MutableBytes,
                       Parameter, ParseLimits, ResultBuffer, Roi, SegmentMetadata, TileMapping,
-                      TileMetadata, TileShape, WorkspaceSpec)
+                      TiffReadLimits, TiffWriteOptions, TileMetadata, TileShape, WorkspaceSpec)
 
 
 class Status(enum.IntEnum):
@@ -190,6 +191,46 @@ def parse_metadata(source, limits: ParseLimits | None = None, size: int | None =
     st = N.lib().ts_parse_metadata(const_bytes(source, size),
                                    C.byref(limits) if limits is not None else None, C.byref(h))
     return Status(st), (ImageMetadata(h.value) if st == 0 else None)
+
+
+class TiffCompression(enum.IntEnum):
+    none = 0
+    deflate = 1
+
+
+def read_tiff(path, limits: TiffReadLimits | None = None):
+    """io::read_tiff: (Status, image) where image is None or a dict with the ImageSpec fields,
+    "pitch_bytes" and "pixels" (a (height, width) uint16 or float32 array)."""
+    h = C.c_void_p(0)
+    st = N.lib().ts_read_tiff(os.fsencode(path), C.byref(limits) if limits is not None else None,
+                              C.byref(h))
+    if st != 0:
+        return Status(st), None
+    try:
+        spec, pitch, data, size = ImageSpec(), C.c_uint64(), C.c_void_p(), C.c_uint64()
+        N.lib().ts_tiff_image_pixels(h.value, C.byref(spec), C.byref(pitch), C.byref(data),
+                                     C.byref(size))
+        raw = np.ctypeslib.as_array(C.cast(data, C.POINTER(C.c_uint8)), (size.value,)).copy()
+    finally:
+        N.lib().ts_tiff_image_destroy(h.value)
+    dtype = np.uint16 if spec.type == PixelType.uint16 else np.float32
+    pixels = raw.view(dtype).reshape(spec.height, spec.width)
+    return Status(st), {"type": PixelType(spec.type), "width": spec.width,
+                        "height": spec.height, "pitch_bytes": pitch.value, "pixels": pixels}
+
+
+def write_tiff(path, image, options: TiffWriteOptions | None = None) -> Status:
+    """io::write_tiff of a host image: a (height, width) uint16 or float32 array, or a
+    ConstImageView of host memory."""
+    if isinstance(image, np.ndarray):
+        arr = np.ascontiguousarray(image)
+        ptype = PixelType.uint16 if arr.dtype == np.uint16 else PixelType.float32
+        v = const_view(arr, ptype, arr.shape[1], arr.shape[0])
+        keep = arr  # noqa: F841  (alive across the call)
+    else:
+        v = image
+    return Status(N.lib().ts_write_tiff(os.fsencode(path), v,
+                                        C.byref(options) if options is not None else None))
 
 
 def version() -> str:

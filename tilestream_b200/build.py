@@ -34,7 +34,7 @@ NVCC_FLAGS = ARCH + ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-ftz=fal
 CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-Wall", "-Wextra", "-ffp-contract=off",
              "-I" + INCLUDE, "-I" + CSRC, "-I" + os.path.join(CUDA_HOME, "include")]
 LINK_FLAGS = ["-shared", "-cudart", "static", "-Xlinker", "-Bsymbolic-functions",
-              "-lpthread", "-ldl", "-lrt"]
+              "-lz", "-lpthread", "-ldl", "-lrt"]
 
 
 def sources():

@@ -5,6 +5,7 @@
 #include <tilestream/info.h>
 #include <tilestream/serve.h>
 #include <tilestream/staging.h>
+#include <tilestream/tiff.h>
 #include <tilestream_c.h>
 
 #include "plan.h"
@@ -35,6 +36,7 @@ TS_SAME_LAYOUT(ts_calibration, ts::cuda::Calibration);
 TS_SAME_LAYOUT(ts_tile_mapping, ts::cuda::TileMapping);
 TS_SAME_LAYOUT(ts_roi_staging, ts::cuda::RoiStaging);
 TS_SAME_LAYOUT(ts_parse_limits, ts::ParseLimits);
+TS_SAME_LAYOUT(ts_tiff_read_limits, ts::io::TiffReadLimits);
 TS_SAME_LAYOUT(ts_workspace_spec, ts::WorkspaceSpec);
 TS_SAME_LAYOUT(ts_tile_metadata, ts::TileMetadata);
 TS_SAME_LAYOUT(ts_segment_metadata, ts::SegmentMetadata);
@@ -82,6 +84,10 @@ struct ts_mixed_batch {
 
 struct ts_plan {
     std::unique_ptr<ts::cuda::BatchPlan> plan;
+};
+
+struct ts_tiff_image {
+    ts::io::TiffImage value;
 };
 
 struct ts_server {
@@ -608,4 +614,58 @@ extern "C" int ts_compress_noalloc(ts_const_image_view input_c, ts_tile_shape ti
     return code(d::cuda_status(
         tsk_encode_static_launch(&image, reinterpret_cast<tsk_result *>(result), stream),
         "allocation-free encode launch"));
+}
+
+extern "C" int ts_read_tiff(const char *path, const ts_tiff_read_limits *limits,
+                            ts_tiff_image **image) {
+    if (image == nullptr) {
+        return code(ts::Status::invalid_argument);
+    }
+    try {
+        auto holder = std::make_unique<ts_tiff_image>();
+        const ts::io::TiffReadLimits l =
+            limits != nullptr ? as<ts::io::TiffReadLimits>(*limits) : ts::io::TiffReadLimits{};
+        const ts::Status st = ts::io::read_tiff(path, holder->value, l);
+        if (st == ts::Status::success) {
+            delete *image;
+            *image = holder.release();
+        }
+        return code(st);
+    } catch (...) {
+        return code(ts::Status::resource_limit);
+    }
+}
+
+extern "C" int ts_tiff_image_pixels(const ts_tiff_image *image, ts_image_spec *spec,
+                                    uint64_t *pitch_bytes, const void **pixels, uint64_t *bytes) {
+    if (image == nullptr || spec == nullptr || pitch_bytes == nullptr || pixels == nullptr ||
+        bytes == nullptr) {
+        return code(ts::Status::invalid_argument);
+    }
+    *spec = as<ts_image_spec>(image->value.image);
+    *pitch_bytes = image->value.pitch_bytes;
+    *pixels = image->value.pixels.data();
+    *bytes = image->value.pixels.size();
+    return 0;
+}
+
+extern "C" void ts_tiff_image_destroy(ts_tiff_image *image) {
+    delete image;
+}
+
+extern "C" int ts_write_tiff(const char *path, ts_const_image_view image,
+                             const ts_tiff_write_options *options) {
+    ts::io::TiffWriteOptions o;
+    if (options != nullptr) {
+        if (options->compression > 1) {
+            return code(ts::Status::invalid_argument);
+        }
+        o.bigtiff = options->bigtiff != 0;
+        o.compression = static_cast<ts::io::TiffCompression>(options->compression);
+        o.horizontal_predictor = options->horizontal_predictor != 0;
+        o.tile_width = options->tile_width;
+        o.tile_height = options->tile_height;
+        o.deflate_level = options->deflate_level;
+    }
+    return code(ts::io::write_tiff(path, as<ts::ConstImageView>(image), o));
 }
