@@ -243,6 +243,18 @@ int ts_compress_noalloc(ts_const_image_view input, ts_tile_shape tile, ts_mutabl
                         ts_device_result *result, void *stream);
 uint64_t ts_compress_noalloc_max_tiles(void);
 
+/* ---- unparsed files (include/tilestream/unparsed.h; extension, no reference counterpart) ---
+ * Whole-image decode of .tsc files in device memory that were never parsed on the host: the
+ * host checks each header from its 64-byte host copy, the decoder validates index entries,
+ * payloads and rows on the device with parse_metadata's rules. At most 16 files per call. */
+typedef struct {
+    ts_const_bytes bytes; /* device memory: the whole file */
+    const void *header;   /* host copy of its first 64 bytes */
+    ts_image_view output; /* device memory */
+} ts_unparsed_file;       /* UnparsedFile */
+int ts_decode_unparsed_async(const ts_unparsed_file *files, uint64_t count,
+                             ts_result_buffer results, void *stream);
+
 /* ---- TIFF import and export (include/tilestream/tiff.h; reference tiff.h:10-37) --------- */
 typedef struct {
     uint32_t max_width, max_height;

@@ -73,6 +73,10 @@ class ParseLimits(C.Structure):
     _fields_ = [("file_bytes", u64), ("tile_count", u64), ("metadata_bytes", u64)]
 
 
+class UnparsedFile(C.Structure):
+    _fields_ = [("bytes", ConstBytes), ("header", C.c_void_p), ("output", ImageView)]
+
+
 class TiffReadLimits(C.Structure):
     _fields_ = [("max_width", u32), ("max_height", u32), ("max_decoded_bytes", u64)]
 
@@ -224,6 +228,7 @@ _SIGNATURES = {
     "ts_roi_staging_size": (C.c_int, [vp, Roi, C.POINTER(RoiStaging)]),
     "ts_stage_roi_tiles": (C.c_int, [vp, Roi, ConstBytes, MutableBytes, C.POINTER(TileMapping),
                                      u64, vp, C.POINTER(RoiStaging)]),
+    "ts_decode_unparsed_async": (C.c_int, [C.POINTER(UnparsedFile), u64, ResultBuffer, vp]),
     "ts_read_tiff": (C.c_int, [C.c_char_p, C.POINTER(TiffReadLimits), C.POINTER(vp)]),
     "ts_tiff_image_pixels": (C.c_int, [vp, C.POINTER(ImageSpec), C.POINTER(u64),
                                        C.POINTER(vp), C.POINTER(u64)]),

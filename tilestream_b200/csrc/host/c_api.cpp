@@ -6,6 +6,7 @@
 #include <tilestream/serve.h>
 #include <tilestream/staging.h>
 #include <tilestream/tiff.h>
+#include <tilestream/unparsed.h>
 #include <tilestream_c.h>
 
 #include "plan.h"
@@ -37,6 +38,8 @@ TS_SAME_LAYOUT(ts_tile_mapping, ts::cuda::TileMapping);
 TS_SAME_LAYOUT(ts_roi_staging, ts::cuda::RoiStaging);
 TS_SAME_LAYOUT(ts_parse_limits, ts::ParseLimits);
 TS_SAME_LAYOUT(ts_tiff_read_limits, ts::io::TiffReadLimits);
+TS_SAME_LAYOUT(ts_unparsed_file, ts::cuda::UnparsedFile);
+static_assert(offsetof(ts_unparsed_file, output) == offsetof(ts::cuda::UnparsedFile, output));
 TS_SAME_LAYOUT(ts_workspace_spec, ts::WorkspaceSpec);
 TS_SAME_LAYOUT(ts_tile_metadata, ts::TileMetadata);
 TS_SAME_LAYOUT(ts_segment_metadata, ts::SegmentMetadata);
@@ -668,4 +671,11 @@ extern "C" int ts_write_tiff(const char *path, ts_const_image_view image,
         o.deflate_level = options->deflate_level;
     }
     return code(ts::io::write_tiff(path, as<ts::ConstImageView>(image), o));
+}
+
+extern "C" int ts_decode_unparsed_async(const ts_unparsed_file *files, uint64_t count,
+                                        ts_result_buffer results, void *stream) {
+    return code(ts::cuda::decode_unparsed_async(
+        reinterpret_cast<const ts::cuda::UnparsedFile *>(files), count,
+        as<ts::cuda::ResultBuffer>(results), static_cast<cudaStream_t>(stream)));
 }

@@ -106,6 +106,13 @@ inline Status view_ok(const ImageView &v) noexcept {
     return view_ok(v.data, v.image, v.pitch_bytes, v.capacity_bytes);
 }
 
+// The parser's header rules and statuses (parse_metadata, after reference
+// src/cpu/parser.cpp:27-84) for a file of `size` bytes whose first 64 bytes are at `header`
+// (size < 64 is malformed_data and reads nothing); on success the image, tile shape and tile
+// count. Defined in parser.cpp.
+Status check_file_header(const std::uint8_t *header, std::uint64_t size, ImageSpec &image,
+                         TileShape &tile, std::uint64_t &tiles) noexcept;
+
 inline std::uint64_t le(const std::uint8_t *p, unsigned n) noexcept {
     std::uint64_t v = 0;
     for (unsigned i = 0; i < n; ++i) {

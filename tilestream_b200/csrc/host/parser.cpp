@@ -300,6 +300,22 @@ Status table_bytes(std::uint64_t tiles, std::uint64_t segments, std::uint64_t &b
 
 } // namespace
 
+namespace host {
+
+Status check_file_header(const std::uint8_t *header, std::uint64_t size, ImageSpec &image,
+                         TileShape &tile, std::uint64_t &tiles) noexcept {
+    Header h;
+    const Status st = read_header(header, size, h);
+    if (st == Status::success) {
+        image = h.image;
+        tile = h.tile;
+        tiles = h.count;
+    }
+    return st;
+}
+
+} // namespace host
+
 Status parse_metadata(ConstBytes source, const ParseLimits &limits,
                       ImageMetadata &metadata) noexcept {
     Status st = host::byte_range(source.data, source.size);

@@ -771,9 +771,12 @@ __device__ __forceinline__ void decode_tile(const Ctx &x, const uint32_t *payloa
 }
 
 // Reads the row descriptors of an encoder-produced tile (decoder.cu:86-110): false when they do
-// not describe exactly the staged payload.
+// not describe exactly the staged payload. The width word is compared whole, so its three
+// reserved bytes must be zero. strict (unparsed files) adds the host parser's remaining row
+// rules (parser.cpp check_payloads, after reference src/cpu/parser.cpp:127-171): a one-column
+// tile has zero-width rows, and the unused high bits of a row's last packed word are zero.
 __device__ bool walk_rows(const uint32_t *payload, uint32_t words, uint32_t width,
-                          uint32_t height, bool f32, uint16_t *rows) {
+                          uint32_t height, bool f32, uint16_t *rows, bool strict) {
     const uint32_t max_bits = f32 ? 32u : 16u;
     uint32_t cursor = 0;
     for (uint32_t r = 0; r < height; ++r) {
@@ -785,8 +788,13 @@ __device__ bool walk_rows(const uint32_t *payload, uint32_t words, uint32_t widt
         if (bits > max_bits || (!f32 && seed > 65535u)) {
             return false;
         }
-        const uint32_t packed = ((width - 1) * bits + 31) / 32;
+        const uint32_t nbits = (width - 1) * bits;
+        const uint32_t packed = (nbits + 31) / 32;
         if (words - cursor - 2 < packed) {
+            return false;
+        }
+        if (strict && ((width == 1 && bits != 0) ||
+                       (nbits % 32 != 0 && (payload[cursor + 1 + packed] >> (nbits % 32)) != 0))) {
             return false;
         }
         rows[r] = static_cast<uint16_t>(cursor);
@@ -914,6 +922,83 @@ struct ServeSource {
     }
 };
 
+// FileSource: unparsed .tsc files (the kernel's parameter block), each decoded whole. Task g is
+// tile l = g - (first task of its file) of its file, in index order. Its index entry and rows
+// are read and validated on the device (TSK_TRUSTED | TSK_UNPARSED), so nothing but the file
+// records is passed. The first task of a file also compares the file's 64 header bytes with
+// the copy the host checked; a difference marks the task (reserved = 1), and staging reports
+// it as malformed data.
+struct FileSource {
+    static constexpr bool kTrusted = true;
+    const tsk_file_batch *batch;
+    uint32_t ntasks;
+    uint32_t cursor; // file of the last task asked for (indexes only increase)
+
+    __device__ tsk_decode_task task(uint32_t g) {
+        const tsk_file *files = batch->files;
+        while (g >= files[cursor].task_end) {
+            ++cursor; // g < ntasks == files[count - 1].task_end ends the walk
+        }
+        const tsk_file &f = files[cursor];
+        const tsk_decode_image &im = f.image;
+        const uint32_t l = g - (cursor != 0 ? files[cursor - 1].task_end : 0u);
+        const uint32_t trow = l / f.tiles_across, tcol = l % f.tiles_across;
+        const uint64_t x = static_cast<uint64_t>(tcol) * im.tile_width;
+        const uint64_t y = static_cast<uint64_t>(trow) * im.tile_height;
+        tsk_decode_task t{};
+        t.src = f.src;
+        t.words_or_tile = l;
+        t.image = cursor;
+        t.width = static_cast<uint16_t>(min(static_cast<uint64_t>(im.tile_width),
+                                            im.archive_width - x));
+        t.height = static_cast<uint16_t>(min(static_cast<uint64_t>(im.tile_height),
+                                             im.archive_height - y));
+        t.row0 = 0;
+        t.row1 = t.height;
+        t.col0 = 0;
+        t.col1 = t.width;
+        t.ox = static_cast<uint32_t>(x);
+        t.oy = static_cast<uint32_t>(y);
+        const uint64_t esize = (f.flags & TSK_F32) ? 4 : 2;
+        t.dst = im.out + y * im.out_pitch + x * esize;
+        t.pitch = im.out_pitch;
+        t.flags = static_cast<uint8_t>(f.flags | TSK_TRUSTED | TSK_UNPARSED |
+                                       (l == 0 ? TSK_FIRST : 0));
+        const bool class_width = t.width == 64 || t.width == 128 || t.width == 256;
+        if (class_width && ((t.dst | t.pitch) & 15u) == 0) {
+            t.flags |= TSK_FULL;
+        }
+        if (l == 0) {
+            const uint32_t *head = reinterpret_cast<const uint32_t *>(f.src);
+            uint32_t diff = 0;
+            for (int k = 0; k < 16; ++k) {
+                diff |= head[k] ^ f.header[k];
+            }
+            t.reserved = diff != 0 ? 1 : 0;
+        }
+        return t;
+    }
+    __device__ uint32_t image_of(uint32_t g) const {
+        uint32_t r = 0;
+        while (r + 1 < batch->count && g >= batch->files[r].task_end) {
+            ++r;
+        }
+        return r;
+    }
+    __device__ const tsk_decode_image &image(uint32_t i) const {
+        return batch->files[i].image;
+    }
+    __device__ void calibration(const tsk_decode_task &, StageHeader &h) const {
+        h.offset = 0.0f; // plain decode only
+        h.gain = 1.0f;
+        h.opitch = h.gpitch = 0;
+        h.omap = h.gmap = 0;
+    }
+    __device__ uint64_t result_bytes(const tsk_decode_task &t) const {
+        return batch->files[t.image].image.result_bytes;
+    }
+};
+
 // Producer: stages one task into stage s.
 template <typename Sh, typename Source>
 __device__ void stage_task(Sh &sh, uint32_t s, const tsk_decode_task &t, const Source &source,
@@ -926,14 +1011,19 @@ __device__ void stage_task(Sh &sh, uint32_t s, const tsk_decode_task &t, const S
     if constexpr (Source::kTrusted) {
         if (t.flags & TSK_TRUSTED) {
             const tsk_decode_image &im = source.image(t.image);
-            const volatile tsk_result *producer =
-                reinterpret_cast<const volatile tsk_result *>(im.encoder_result);
-            const uint32_t produced_status = producer->status;
-            const uint64_t produced_bytes = producer->bytes_written;
+            const bool unparsed = (t.flags & TSK_UNPARSED) != 0;
+            uint32_t produced_status = 0;
+            uint64_t end = im.capacity; // unparsed: the file size
+            if (!unparsed) {
+                const volatile tsk_result *producer =
+                    reinterpret_cast<const volatile tsk_result *>(im.encoder_result);
+                produced_status = producer->status;
+                const uint64_t produced_bytes = producer->bytes_written;
+                end = produced_bytes < im.capacity ? produced_bytes : im.capacity;
+            }
             if (produced_status != 0) {
                 state = kStageSkip;
             } else {
-                const uint64_t end = produced_bytes < im.capacity ? produced_bytes : im.capacity;
                 // The archive is only 4-byte aligned: read the entry as 32-bit words.
                 const uint32_t *e = reinterpret_cast<const uint32_t *>(t.src + 64 +
                                                                        32 * t.words_or_tile);
@@ -945,9 +1035,27 @@ __device__ void stage_task(Sh &sh, uint32_t s, const tsk_decode_task &t, const S
                 const uint64_t raw =
                     (static_cast<uint64_t>(t.width) * t.height * s_bytes + 3) / 4 * 4;
                 mode = e0 & 0xffu;
-                if (mode > TSK_PREDICT || ew != t.width || eh != t.height || offset % 4 != 0 ||
-                    length % 4 != 0 || length == 0 || length > raw || offset > end ||
-                    length > end - offset) {
+                bool bad = mode > TSK_PREDICT || ew != t.width || eh != t.height ||
+                           offset % 4 != 0 || length % 4 != 0 || length == 0 || length > raw ||
+                           offset > end || length > end - offset;
+                if (unparsed) {
+                    // The host parser's other index rules (parser.cpp check_index, after
+                    // reference src/cpu/parser.cpp:86-126): reserved bytes zero, RAW and
+                    // CONSTANT lengths exact, payloads chained from the end of the index to the
+                    // end of the file; and the header the host checked.
+                    const uint64_t tile = t.words_or_tile;
+                    uint64_t expected = 64 + 32ull * im.tile_count;
+                    if (tile != 0) {
+                        expected = (e[-6] | (static_cast<uint64_t>(e[-5]) << 32)) +
+                                   (e[-4] | (static_cast<uint64_t>(e[-3]) << 32));
+                    }
+                    bad = bad || (e0 >> 8) != 0 || e[6] != 0 || e[7] != 0 || offset != expected ||
+                          (mode == TSK_RAW && length != raw) ||
+                          (mode == TSK_CONSTANT && length != 4) ||
+                          (tile + 1 == im.tile_count && !bad && offset + length != end) ||
+                          t.reserved != 0;
+                }
+                if (bad) {
                     state = kStageMalformed;
                 } else {
                     src = t.src + offset;
@@ -1017,10 +1125,22 @@ __device__ __forceinline__ void consume_tile(Sh &sh, uint32_t s, const Source &s
     const bool f32 = (t.flags & TSK_F32) != 0;
     const bool calibrated = (t.flags & TSK_CALIBRATED) != 0;
     const bool trusted = (t.flags & TSK_TRUSTED) != 0;
+    const bool unparsed = (t.flags & TSK_UNPARSED) != 0;
     bool ok = state == kStageOk;
-    if (trusted && ok && hmode == TSK_PREDICT) {
+    if (trusted && ok && (hmode == TSK_PREDICT || unparsed)) {
         if (lead) {
-            sh.valid[s] = walk_rows(payload, h.words, t.width, t.height, f32, sh.rows[s]);
+            bool valid;
+            if (hmode == TSK_PREDICT) {
+                valid = walk_rows(payload, h.words, t.width, t.height, f32, sh.rows[s], unparsed);
+            } else if (hmode == TSK_RAW) {
+                // The bytes after the last sample are zero.
+                const uint32_t tail = (static_cast<uint32_t>(t.width) * t.height * 2u) % 4u;
+                valid = f32 || tail == 0 || (payload[h.words - 1] >> 16) == 0;
+            } else {
+                // A uint16 constant fills the low half of its word.
+                valid = f32 || (payload[0] >> 16) == 0;
+            }
+            sh.valid[s] = valid;
         }
         if constexpr (RW == 1) {
             __syncwarp();
@@ -1093,8 +1213,10 @@ __device__ __forceinline__ void consume_tile(Sh &sh, uint32_t s, const Source &s
                     uint32_t status =
                         *reinterpret_cast<volatile uint32_t *>(&results[t.image].status);
                     const uint32_t produced =
-                        reinterpret_cast<const volatile tsk_result *>(im.encoder_result)
-                            ->status;
+                        im.encoder_result != 0
+                            ? reinterpret_cast<const volatile tsk_result *>(im.encoder_result)
+                                  ->status
+                            : 0u;
                     if (produced != 0) {
                         status = produced;
                     }
@@ -1315,6 +1437,16 @@ __global__ void __launch_bounds__(threads_of(CW), MinBlocks)
     decode_body<MaxPayload, Stages, Paths, CW, G16, 0, CW>(source, rowtab, results, one, top);
 }
 
+// A batch of unparsed files: the files arrive in the parameter block.
+template <uint32_t MaxPayload, uint32_t Stages, uint32_t Paths, uint32_t CW, uint32_t G16,
+          uint32_t MinBlocks, uint32_t NR, uint32_t RW>
+__global__ void __launch_bounds__(threads_of(CW), MinBlocks)
+    file_kernel(const __grid_constant__ tsk_file_batch batch, tsk_result *results, uint32_t one,
+                uint32_t top) {
+    FileSource source{&batch, batch.ntasks, 0};
+    decode_body<MaxPayload, Stages, Paths, CW, G16, NR, RW>(source, nullptr, results, one, top);
+}
+
 using KernelFn = void (*)(const tsk_decode_task *, uint32_t, const tsk_decode_image *,
                           const tsk_row_start *, tsk_result *, uint32_t, uint32_t);
 
@@ -1446,6 +1578,26 @@ ServeVariant select_serve(bool all_u16) {
     }
     return {serve_kernel<16384, 3, kU16 | kF32 | kPlain | kCal, 8, 8, 3>,
             sizeof(Shared<16384, 3>), threads_of(8)};
+}
+
+using FileFn = void (*)(tsk_file_batch, tsk_result *, uint32_t, uint32_t);
+
+struct FileVariant {
+    FileFn fn;
+    size_t smem;
+    uint32_t threads;
+};
+
+// Unparsed-file instances, plain decode: uint16 files in the default plain uint16 shape (4
+// warps x 16 columns in warp pairs, single-pass rows, 4 stages of 8 KiB, 5 CTAs per SM), and
+// batches with FP32 files in the mixed batch's shape 5 (two 16 KiB stages, 5 CTAs per SM).
+FileVariant select_file(bool any_f32) {
+    if (!any_f32) {
+        return {file_kernel<8192, 4, kU16 | kPlain, 4, 16, 5, 1, 2>, sizeof(Shared<8192, 4>),
+                threads_of(4)};
+    }
+    return {file_kernel<16384, 2, kU16 | kF32 | kPlain, 4, 16, 5, 1, 4>,
+            sizeof(Shared<16384, 2>), threads_of(4)};
 }
 
 } // namespace
@@ -1606,5 +1758,51 @@ extern "C" int tsk_serve_launch(const tsk_serve_batch *batch, const tsk_serve_ar
     const tsk::ServeVariant v = tsk::select_serve(all_u16 != 0);
     const uint32_t blocks = grid < batch->ntasks ? grid : batch->ntasks;
     v.fn<<<blocks, v.threads, v.smem, stream>>>(*batch, archives, rows, results, 1u, 0x80000000u);
+    return cudaGetLastError();
+}
+
+extern "C" int tsk_file_prepare(int any_f32, int device, uint32_t *grid) {
+    const tsk::FileVariant v = tsk::select_file(any_f32 != 0);
+    const void *key = reinterpret_cast<const void *>(v.fn);
+    int per_sm = 0, sms = 0;
+    {
+        std::lock_guard<std::mutex> lock(g_prepared_mutex);
+        for (int i = 0; i < g_prepared_count; ++i) {
+            if (g_prepared[i].device == device && g_prepared[i].fn == key) {
+                per_sm = g_prepared[i].per_sm;
+                sms = g_prepared[i].sms;
+                break;
+            }
+        }
+    }
+    if (sms == 0) {
+        cudaError_t e = cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             static_cast<int>(v.smem));
+        if (e != cudaSuccess) return e;
+        e = cudaFuncSetAttribute(v.fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 cudaSharedmemCarveoutMaxShared);
+        if (e != cudaSuccess) return e;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v.fn, v.threads, v.smem);
+        if (e != cudaSuccess) return e;
+        e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        if (e != cudaSuccess) return e;
+        std::lock_guard<std::mutex> lock(g_prepared_mutex);
+        if (g_prepared_count < kPreparedSlots) {
+            g_prepared[g_prepared_count++] = {device, key, per_sm, sms};
+        }
+    }
+    *grid = static_cast<uint32_t>(sms) * static_cast<uint32_t>(per_sm < 1 ? 1 : per_sm);
+    return cudaSuccess;
+}
+
+extern "C" int tsk_file_launch(const tsk_file_batch *batch, tsk_result *results, uint32_t grid,
+                               int any_f32, cudaStream_t stream) {
+    if (batch->count == 0) return cudaSuccess;
+    // Validation counts each file's finished tiles in its record: the records start cleared.
+    cudaError_t e = cudaMemsetAsync(results, 0, sizeof(tsk_result) * batch->count, stream);
+    if (e != cudaSuccess || batch->ntasks == 0) return e;
+    const tsk::FileVariant v = tsk::select_file(any_f32 != 0);
+    const uint32_t blocks = grid < batch->ntasks ? grid : batch->ntasks;
+    v.fn<<<blocks, v.threads, v.smem, stream>>>(*batch, results, 1u, 0x80000000u);
     return cudaGetLastError();
 }

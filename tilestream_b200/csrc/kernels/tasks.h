@@ -26,6 +26,8 @@ enum {
     TSK_TRUSTED = 4,    // index entry and rows are read on the device (encoder output)
     TSK_FIRST = 8,      // first task of its image: writes the image's result record
     TSK_FULL = 16,      // every column of full-width rows is written, to 16-byte-aligned rows
+    TSK_UNPARSED = 32,  // with TSK_TRUSTED: a file never parsed on the host, validated on the
+                        // device with the host parser's rules (no producing result record)
 };
 
 // Largest payload of one tile: RAW FP32, 4096 samples.
@@ -176,6 +178,31 @@ typedef struct __align__(16) {
     tsk_serve_request requests[TSK_SERVE_MAX_BATCH];
 } tsk_serve_batch;
 
+// --- unparsed files: whole-image decode of .tsc files validated on the device ---------------
+
+// One file. Its tasks (one per tile, in index order) are derived on the device; the index
+// entries and row descriptors are read and validated there. image.capacity is the file size,
+// image.encoder_result 0, image.tile_count the file's tiles. 192 bytes.
+typedef struct __align__(16) {
+    tsk_decode_image image;
+    uint64_t src;         // device address of the file
+    uint32_t task_end;    // tasks of the batch up to and including this file
+    uint32_t tiles_across;
+    uint32_t flags;       // TSK_F32 or 0
+    uint32_t reserved;
+    uint32_t header[16];  // the host-checked first 64 bytes the device bytes must hold
+} tsk_file;
+
+// A batch of files, passed as the kernel's parameter block (3,088 bytes: below the classic 4 KB
+// limit).
+#define TSK_FILE_MAX_BATCH 16
+typedef struct __align__(16) {
+    uint32_t count;
+    uint32_t ntasks; // files[count - 1].task_end
+    uint32_t reserved[2];
+    tsk_file files[TSK_FILE_MAX_BATCH];
+} tsk_file_batch;
+
 // DeviceResult as seen by the kernels (types.h: {status, reserved, bytes_written}).
 typedef struct {
     uint32_t status;
@@ -207,6 +234,12 @@ int tsk_serve_launch(const tsk_serve_batch *batch, const tsk_serve_archive *arch
                      cudaStream_t stream);
 // Loads the serving kernel instance and returns its persistent grid (SMs x resident CTAs).
 int tsk_serve_prepare(int all_u16, int device, uint32_t *grid);
+// Decodes a batch of unparsed files (clearing their result records first, which the
+// validation's completion count needs).
+int tsk_file_launch(const tsk_file_batch *batch, tsk_result *results, uint32_t grid,
+                    int any_f32, cudaStream_t stream);
+// Loads the unparsed-file kernel instance and returns its persistent grid.
+int tsk_file_prepare(int any_f32, int device, uint32_t *grid);
 
 // Encodes every tile of every image in one pass. state: tsk_encode_state_bytes(total_tiles)
 // bytes of workspace, cleared by the launcher in stream order.

@@ -159,6 +159,29 @@ class MixedBatch:
             self.handle = None
 
 
+# ---- unparsed files (include/tilestream/unparsed.h) -------------------------------------------
+
+MAX_UNPARSED_FILES = 16
+
+
+def decode_unparsed_async(files, results, stream=None) -> Status:
+    """Whole-image decode of .tsc files never parsed on the host. files: a sequence of
+    (device ConstBytes of the whole file, host copy of its first 64 bytes (bytes or uint8
+    array), ImageView of the device output). results: ResultBuffer or a device buffer."""
+    files = list(files)
+    arr = (N.UnparsedFile * max(1, len(files)))()
+    keep = []
+    for k, (src, header, out) in enumerate(files):
+        head = C.create_string_buffer(bytes(header[:64]) if len(header) >= 64 else bytes(header),
+                                      64)
+        keep.append(head)
+        arr[k].bytes = src
+        arr[k].header = C.cast(head, C.c_void_p)
+        arr[k].output = out
+    return Status(N.lib().ts_decode_unparsed_async(arr, len(files), _results(results),
+                                                   stream_handle(stream)))
+
+
 def decode_shape_count() -> int:
     return int(N.lib().ts_decode_shape_count())
 
