@@ -365,8 +365,46 @@ def run_ours(args, rank, world, device, torch, dist):
             "file_bytes": len(s["file"]),
         }
 
+    # The same step from unparsed files (decode_unparsed_async: the three archives in one launch,
+    # index entries, payloads and rows validated on the device), device time per step.
+    unparsed_results = torch.zeros(16 * 3, dtype=torch.uint8, device="cuda")
+
+    def unparsed_pass():
+        for slot in range(copies):
+            entries = [(api.ConstBytes(s["copies"][slot]["src"].data_ptr(), len(s["file"])),
+                        s["file"][:64], api.view(s["copies"][slot]["out"], 1, W, H, W * 2))
+                       for s in shapes]
+            st = cuda.decode_unparsed_async(
+                entries, api.ResultBuffer(unparsed_results.data_ptr(), 3), stream)
+            assert st == 0, st
+    g = None
+    if graphs is not None:
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=stream, capture_error_mode="relaxed"):
+            unparsed_pass()
+    run_pass = g.replay if g is not None else unparsed_pass
+    for _ in range(3):
+        run_pass()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(20):
+        run_pass()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    unparsed_step_ms = e0.elapsed_time(e1) / (20 * copies)
+    recs_u = unparsed_results.cpu().numpy().view(np.uint64).reshape(-1, 2)
+    assert all(int(r[0]) == 0 and int(r[1]) == W * H * 2 for r in recs_u), recs_u
+
     peak, peak_src = measured_peaks()
     alg_per_launch = sum(s["algorithmic"] for s in shapes) # one launch per step
+    unparsed = {"workload": "the headline step from unparsed files: the three archives in one "
+                            "decode_unparsed_async launch (a result-record clear and the decode), "
+                            "validation on the device",
+                "step_us": round(unparsed_step_ms * 1e3, 2),
+                "decoded_gbs": round(decoded_per_step / unparsed_step_ms / 1e6, 1),
+                "roofline_frac": round(alg_per_launch / (unparsed_step_ms / 1e3) / 1e9 / peak, 4),
+                "cuda_graph": g is not None}
     launch_ms = step_ms
     achieved = alg_per_launch / (launch_ms / 1e3) / 1e9
 
@@ -391,6 +429,7 @@ def run_ours(args, rank, world, device, torch, dist):
         "graph_steps": cycle_steps if cycles is not None else 1,
         **({"graph_capture_error": capture_error} if capture_error else {}),
         "per_shape": per_shape,
+        "unparsed_decode": unparsed,
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                      "peak_source": peak_src, "unit": "GB/s", "frac": round(achieved / peak, 4),
                      "algorithmic_bytes_per_launch": int(alg_per_launch),
@@ -1246,6 +1285,26 @@ def run_batched(args, torch, stream, peak):
     torch.cuda.synchronize()
     batched_ms = e0.elapsed_time(e1) / steps
 
+    # The device work queue against static striding: the same batch with fixed kernel shapes,
+    # static (5, 6) and with the work queue (8, 9: the same shapes claiming task chunks).
+    def fixed_ms(shape):
+        st_f, b = cuda.prepare_mixed_batch(entries, results, stream, graph=True, shape=shape)
+        assert st_f == Status.success, st_f
+        for _ in range(args.warmup):
+            b.run(stream)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(steps):
+            b.run(stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+    queue = {}
+    for static, dynamic in ((5, 8), (6, 9)):
+        a, b = fixed_ms(static), fixed_ms(dynamic)
+        queue[f"shape{static}_static_ms"] = round(a, 4)
+        queue[f"shape{dynamic}_work_queue_ms"] = round(b, 4)
+
     ws = torch.empty(max(max(p[0].workspace_bytes() for p in plans), 256), dtype=torch.uint8,
                      device="cuda")
     res1 = torch.zeros(16, dtype=torch.uint8, device="cuda")
@@ -1279,6 +1338,7 @@ def run_batched(args, torch, stream, peak):
                                 "decoded_gbs": round(decoded_bytes / graphed_ms / 1e6, 1)},
             "speedup_vs_per_image_eager": round(eager_ms / batched_ms, 2),
             "speedup_vs_per_image_graph": round(graphed_ms / batched_ms, 2),
+            "work_queue_vs_static": queue,
             "bit_exact": exact}
 
 

@@ -163,15 +163,18 @@ def test_every_kernel_shape_matches_oracle(cuda_ready, oracle_lib, f32):
     items, keep, checks = plain_items(oracle_lib, list(range(13005000, 13005060)), f32)
     assert any(op == cuda.Operation.decode_roi for op, _ in items)
     for shape in range(cuda.decode_shape_count()):
-        results = device_bytes(16 * len(items), fill=0xFF)
-        for out, pitch, row_bytes, rh, want, nbytes in checks:
-            out.fill_(SENTINEL)
-        st, batch = cuda.prepare_mixed_batch(items, results, stream, shape=shape)
-        assert st == Status.success, (shape, st)
-        assert batch.stats()["shape"] == shape
-        assert batch.run(stream) == Status.success
-        torch.cuda.synchronize()
-        verify_plain(checks, results)
+        for graph in (True, False):
+            results = device_bytes(16 * len(items), fill=0xFF)
+            for out, pitch, row_bytes, rh, want, nbytes in checks:
+                out.fill_(SENTINEL)
+            st, batch = cuda.prepare_mixed_batch(items, results, stream, shape=shape, graph=graph)
+            assert st == Status.success, (shape, st)
+            assert batch.stats()["shape"] == shape
+            # Twice: shapes with the device work queue clear its counter before every launch.
+            assert batch.run(stream) == Status.success
+            assert batch.run(stream) == Status.success
+            torch.cuda.synchronize()
+            verify_plain(checks, results)
     st, _ = cuda.prepare_mixed_batch(items, device_bytes(16 * len(items)), stream,
                                      shape=cuda.decode_shape_count())
     assert st == Status.invalid_argument

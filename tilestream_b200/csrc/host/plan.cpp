@@ -738,11 +738,16 @@ Status finalize(Operation operation, Draft &d, PlanState &plan, cudaStream_t str
     }
 
     std::uint64_t total = 0, at_images = 0, at_tasks = 0, at_rows = 0, at_enc = 0, at_cal_images = 0,
-                  at_cal_tasks = 0;
+                  at_cal_tasks = 0, at_claims = 0;
+    const std::vector<std::uint32_t> claims(operation == Operation::compress ||
+                                                    operation == Operation::calibrate
+                                                ? 0
+                                                : 1,
+                                            0u); // the decode work queue's counter
     if (!place(total, d.images, at_images) || !place(total, d.tasks, at_tasks) ||
         !place(total, d.rows, at_rows) || !place(total, d.encode_images, at_enc) ||
         !place(total, d.calib_images, at_cal_images) ||
-        !place(total, d.calib_tasks, at_cal_tasks)) {
+        !place(total, d.calib_tasks, at_cal_tasks) || !place(total, claims, at_claims)) {
         return Status::size_overflow;
     }
     if (cudaMallocAsync(&plan.storage, static_cast<std::size_t>(total), stream) != cudaSuccess) {
@@ -760,6 +765,7 @@ Status finalize(Operation operation, Draft &d, PlanState &plan, cudaStream_t str
     plan.calib_images = reinterpret_cast<const tsk_calib_image *>(dev + at_cal_images);
     plan.calib_tasks = reinterpret_cast<const tsk_calib_task *>(dev + at_cal_tasks);
     plan.calib_task_count = static_cast<std::uint32_t>(d.calib_tasks.size());
+    plan.claims = claims.empty() ? nullptr : reinterpret_cast<std::uint32_t *>(dev + at_claims);
 
     // Load every kernel the plan launches now, so no execution has to (docs/api.md:69).
     int err = 0;
@@ -791,6 +797,7 @@ Status finalize(Operation operation, Draft &d, PlanState &plan, cudaStream_t str
         pack(image, at_enc, d.encode_images);
         pack(image, at_cal_images, d.calib_images);
         pack(image, at_cal_tasks, d.calib_tasks);
+        pack(image, at_claims, claims);
         if ((total != 0 && cudaMemcpyAsync(plan.storage, image.data(),
                                            static_cast<std::size_t>(total),
                                            cudaMemcpyHostToDevice, stream) != cudaSuccess) ||
@@ -970,7 +977,8 @@ Status run_decode(const BatchPlan &plan, Operation op, MutableBytes workspace,
         return detail::cuda_failure("cudaMemsetAsync (results)");
     }
     return detail::cuda_status(
-        tsk_decode_launch(p->tasks, p->task_count, p->images, p->rows, records, p->config, stream),
+        tsk_decode_launch(p->tasks, p->task_count, p->images, p->rows, records, p->config,
+                          p->claims, stream),
         "decode launch");
 }
 
@@ -1058,7 +1066,7 @@ cudaError_t enqueue_decode(const detail::PlanState &p, tsk_result *results, cuda
         if (e != cudaSuccess) return e;
     }
     return static_cast<cudaError_t>(tsk_decode_launch(p.tasks, p.task_count, p.images, p.rows,
-                                                      results, p.config, stream));
+                                                      results, p.config, p.claims, stream));
 }
 
 // The tuner's memory: workload key -> (shape, resident CTAs per SM).
@@ -1136,14 +1144,17 @@ Status autotune(detail::PlanState &p, tsk_result *results, const char *cache, cu
     if (hit != g_tune_memo.end()) {
         return detail::cuda_status(apply(hit->second.shape, hit->second.per_sm), "tuned config");
     }
-    // The kernel shapes of the batch's instance (kernels/decode.cu, select): eight for plain
-    // uint16, four for plain mixed uint16 + FP32, two for the others.
+    // The kernel shapes of the batch's instance (kernels/decode.cu, select): nineteen for plain
+    // uint16, ten for plain mixed uint16 + FP32, two for the others.
     const bool plain_u16 = p.config.paths == (TSK_PATH_U16 | TSK_PATH_PLAIN);
     const bool plain_mixed = p.config.paths == (TSK_PATH_U16 | TSK_PATH_F32 | TSK_PATH_PLAIN);
-    const std::uint32_t shapes_all[TSK_DECODE_SHAPES] = {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15, 16, 17},
-                        shapes_mixed[] = {0, 1, 2, 3, 4, 5, 6, 7}, shapes_two[] = {0, 2};
+    const std::uint32_t shapes_all[TSK_DECODE_SHAPES] = {0,  1,  2,  3,  4,  5,  6,  7,  8,  9,
+                                                         10, 11, 12, 13, 14, 15, 16, 17, 18},
+                        shapes_mixed[] = {0, 1, 2, 3, 4, 5, 6, 7, 8, 9}, shapes_two[] = {0, 2};
     const std::uint32_t *shapes = plain_u16 ? shapes_all : plain_mixed ? shapes_mixed : shapes_two;
-    const std::size_t nshapes = plain_u16 ? TSK_DECODE_SHAPES : plain_mixed ? 8 : 2;
+    const std::size_t nshapes = plain_u16 ? TSK_DECODE_SHAPES
+                                : plain_mixed ? sizeof(shapes_mixed) / sizeof(shapes_mixed[0])
+                                              : 2;
     cudaEvent_t start = nullptr, stop = nullptr;
     if (cudaEventCreate(&start) != cudaSuccess || cudaEventCreate(&stop) != cudaSuccess) {
         return detail::cuda_failure("cudaEventCreate");
@@ -1263,8 +1274,8 @@ Status prepare_mixed_batch(const MixedItem *items, std::uint64_t count, ResultBu
             if (options.graph) {
                 const int e = tsk_decode_graph(plan.tasks, plan.task_count, plan.images, plan.rows,
                                                impl->results, static_cast<std::uint32_t>(count),
-                                               plan.trusted ? 1 : 0, plan.config, &impl->graph,
-                                               &impl->exec);
+                                               plan.trusted ? 1 : 0, plan.config, plan.claims,
+                                               &impl->graph, &impl->exec);
                 if (e != 0) {
                     impl->graph = nullptr;
                     impl->exec = nullptr;

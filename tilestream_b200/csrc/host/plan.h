@@ -76,6 +76,7 @@ struct PlanState {
     const tsk_decode_image *images = nullptr;
     const tsk_row_start *rows = nullptr;
     tsk_decode_config config{};
+    std::uint32_t *claims = nullptr; // the work queue's counter (dynamic kernel shapes)
     bool trusted = false;
 
     // Encode.

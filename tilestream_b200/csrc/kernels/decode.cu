@@ -44,7 +44,7 @@ constexpr uint32_t threads_of(uint32_t cw, bool self = false) {
     return cw * 32 + (self ? 0 : 32);
 }
 
-enum : uint32_t { kStageOk = 0, kStageSkip = 1, kStageMalformed = 2 };
+enum : uint32_t { kStageOk = 0, kStageSkip = 1, kStageMalformed = 2, kStageEnd = 3 };
 
 // Everything the consumers need about one staged tile, written by the producer.
 struct StageHeader {
@@ -56,7 +56,7 @@ struct StageHeader {
     uint32_t shift; // byte offset of payload word 0 within the stage buffer
     uint32_t words; // payload words
     uint32_t mode;
-    uint32_t state; // kStageOk / kStageSkip / kStageMalformed
+    uint32_t state; // kStageOk / kStageSkip / kStageMalformed / kStageEnd (no more tasks)
 };
 
 // MaxPayload: the largest tile payload of the plan (8 KiB for uint16-only plans, 16 KiB with
@@ -829,6 +829,7 @@ struct TableSource {
     const tsk_decode_task *tasks;
     const tsk_decode_image *images;
     uint32_t ntasks;
+    uint32_t *claims; // the device work queue's counter (dynamic instances), else unused
 
     __device__ tsk_decode_task task(uint32_t g) {
         return load_task(tasks + g);
@@ -1239,8 +1240,13 @@ __device__ __forceinline__ void consume_tile(Sh &sh, uint32_t s, const Source &s
 // g + CW / RW, ..., each of its warps a slice of the tile's rows, and the group releases the
 // tile's stage. RW = CW: every warp works on every tile; smaller groups run a tile's set-up
 // fewer times per tile.
+//
+// Dyn: the device work queue. Instead of the static stride, the producer claims chunks of kChunk
+// consecutive tasks from a counter in device memory (cleared before the launch), one chunk
+// ahead, so CTAs that drew cheap tiles take more of them; after the last task it stages one end
+// marker per consumer group.
 template <uint32_t MaxPayload, uint32_t Stages, uint32_t Paths, uint32_t CW, uint32_t G16,
-          uint32_t NR, uint32_t RW, typename Source>
+          uint32_t NR, uint32_t RW, bool Dyn = false, typename Source>
 __device__ __forceinline__ void decode_body(Source &source, const tsk_row_start *rowtab,
                                             tsk_result *results, uint32_t one, uint32_t top) {
     using Sh = Shared<MaxPayload, Stages>;
@@ -1274,6 +1280,50 @@ __device__ __forceinline__ void decode_body(Source &source, const tsk_row_start 
         // so the first stages fill while that grid finishes. Encoder output may be that grid's
         // product: the first trusted task waits for it (griddep_wait) before it is staged.
         if (lane != 0) {
+            return;
+        }
+        if constexpr (Dyn) {
+            constexpr uint32_t kChunk = 4;
+            uint32_t g = atomicAdd(source.claims, kChunk);
+            uint32_t end = g + kChunk < ntasks ? g + kChunk : ntasks;
+            uint32_t ahead = g < ntasks ? atomicAdd(source.claims, kChunk) : ntasks;
+            tsk_decode_task t{};
+            if (g < ntasks) {
+                t = source.task(g);
+            }
+            bool waited = false;
+            uint32_t i = 0;
+            for (; g < ntasks; ++i) {
+                const uint32_t s = i % Stages;
+                uint32_t ng = g + 1;
+                if (ng >= end) {
+                    ng = ahead;
+                    end = ng + kChunk < ntasks ? ng + kChunk : ntasks;
+                    ahead = ng < ntasks ? atomicAdd(source.claims, kChunk) : ntasks;
+                }
+                tsk_decode_task next{};
+                if (ng < ntasks) {
+                    next = source.task(ng);
+                }
+                if (i >= Stages && !mbar_wait(&sh.empty[s], ((i / Stages) - 1) & 1u)) {
+                    return; // consumers stopped; they have reported the timeout
+                }
+                if (!waited && (t.flags & TSK_TRUSTED)) {
+                    griddep_wait();
+                    waited = true;
+                }
+                stage_task(sh, s, t, source, rowtab);
+                t = next;
+                g = ng;
+            }
+            for (uint32_t k = 0; k < kGroups; ++k, ++i) {
+                const uint32_t s = i % Stages;
+                if (i >= Stages && !mbar_wait(&sh.empty[s], ((i / Stages) - 1) & 1u)) {
+                    return;
+                }
+                sh.header[s].state = kStageEnd;
+                mbar_arrive(&sh.full[s]);
+            }
             return;
         }
         tsk_decode_task t{};
@@ -1310,13 +1360,21 @@ __device__ __forceinline__ void decode_body(Source &source, const tsk_row_start 
     // The thread that walks trusted rows and writes result records for this group's tiles.
     const uint32_t group = warp / RW, slot = warp % RW;
     const bool lead = lane == 0 && slot == 0;
-    for (uint32_t i = group; i < mine; i += kGroups) {
+    uint32_t last_image = 0; // Dyn: the image a timeout is reported on
+    for (uint32_t i = group; Dyn || i < mine; i += kGroups) {
         const uint32_t s = i % Stages;
         if (!mbar_wait(&sh.full[s], (i / Stages) & 1u)) {
             if (lead) {
-                fail(results, source.image_of(blockIdx.x + i * gridDim.x), 9u); // cuda_error
+                fail(results, Dyn ? last_image : source.image_of(blockIdx.x + i * gridDim.x),
+                     9u); // cuda_error
             }
             return;
+        }
+        if constexpr (Dyn) {
+            if (sh.header[s].state == kStageEnd) {
+                return;
+            }
+            last_image = sh.header[s].task.image;
         }
         consume_tile<Paths, RW, G16, NR, true>(sh, s, source, results, one, top, lead, slot,
                                                group);
@@ -1409,19 +1467,19 @@ __device__ __forceinline__ void decode_body_self(Source &source, const tsk_row_s
 
 // A planned queue (every plan and mixed batch); MinBlocks resident CTAs per SM.
 template <uint32_t MaxPayload, uint32_t Stages, uint32_t Paths, uint32_t CW, uint32_t G16,
-          uint32_t MinBlocks, uint32_t NR, uint32_t RW, bool Self>
+          uint32_t MinBlocks, uint32_t NR, uint32_t RW, bool Self, bool Dyn>
 __global__ void __launch_bounds__(threads_of(CW, Self), MinBlocks)
     decode_kernel(const tsk_decode_task *__restrict__ tasks, uint32_t ntasks,
                   const tsk_decode_image *__restrict__ images,
                   const tsk_row_start *__restrict__ rowtab, tsk_result *results, uint32_t one,
-                  uint32_t top) {
-    TableSource source{tasks, images, ntasks};
+                  uint32_t top, uint32_t *claims) {
+    TableSource source{tasks, images, ntasks, claims};
     if constexpr (Self) {
         decode_body_self<MaxPayload, Stages, Paths, CW, G16, NR, RW>(source, rowtab, results, one,
                                                                       top);
     } else {
-        decode_body<MaxPayload, Stages, Paths, CW, G16, NR, RW>(source, rowtab, results, one,
-                                                                 top);
+        decode_body<MaxPayload, Stages, Paths, CW, G16, NR, RW, Dyn>(source, rowtab, results,
+                                                                      one, top);
     }
 }
 
@@ -1448,12 +1506,13 @@ __global__ void __launch_bounds__(threads_of(CW), MinBlocks)
 }
 
 using KernelFn = void (*)(const tsk_decode_task *, uint32_t, const tsk_decode_image *,
-                          const tsk_row_start *, tsk_result *, uint32_t, uint32_t);
+                          const tsk_row_start *, tsk_result *, uint32_t, uint32_t, uint32_t *);
 
 struct Variant {
     KernelFn fn;
     size_t smem;
     uint32_t threads;
+    bool dynamic; // claims tasks from the work-queue counter (cleared before each launch)
 };
 
 // Kernel instances: uint16-only plans stage 8 KiB tiles (four stages), plans with FP32 stage
@@ -1462,10 +1521,10 @@ struct Variant {
 // headline one, comes in four shapes (consumer warps x columns per lane) for the tuner.
 template <uint32_t MaxPayload, uint32_t Stages, uint32_t Paths, uint32_t CW = 8,
           uint32_t G16 = 8, uint32_t MinBlocks = 3, uint32_t NR = 0, uint32_t RW = CW,
-          bool Self = false>
+          bool Self = false, bool Dyn = false>
 Variant make() {
-    return {decode_kernel<MaxPayload, Stages, Paths, CW, G16, MinBlocks, NR, RW, Self>,
-            sizeof(Shared<MaxPayload, Stages>), threads_of(CW, Self)};
+    return {decode_kernel<MaxPayload, Stages, Paths, CW, G16, MinBlocks, NR, RW, Self, Dyn>,
+            sizeof(Shared<MaxPayload, Stages>), threads_of(CW, Self), Dyn};
 }
 
 // Shapes of the plain uint16 instance (consumer warps x uint16 columns per lane, stages,
@@ -1515,6 +1574,8 @@ Variant select(uint32_t paths, uint32_t shape) {
                 return make<8192, 4, kU16 | kPlain, 4, 16, 4, 2, 2, true>();
             case 17:
                 return make<8192, 8, kU16 | kPlain, 4, 16, 3, 1, 1, true>();
+            case 18: // shape 13 with the device work queue
+                return make<8192, 4, kU16 | kPlain, 4, 16, 5, 1, 2, false, true>();
             default:
                 return make<8192, 4, kU16 | kPlain, 8, 8, 4>();
             }
@@ -1551,6 +1612,10 @@ Variant select(uint32_t paths, uint32_t shape) {
             return make<16384, 3, kU16 | kF32 | kPlain, 4, 16, 4, 1>();
         case 7: // shape 5 with six CTAs per SM
             return make<16384, 2, kU16 | kF32 | kPlain, 4, 16, 6, 1>();
+        case 8: // shape 5 with the device work queue
+            return make<16384, 2, kU16 | kF32 | kPlain, 4, 16, 5, 1, 4, false, true>();
+        case 9: // shape 6 with the device work queue
+            return make<16384, 3, kU16 | kF32 | kPlain, 4, 16, 4, 1, 4, false, true>();
         default:
             return narrow ? make<16384, 3, kU16 | kF32 | kPlain, 4, 16, 4>()
                           : make<16384, 3, kU16 | kF32 | kPlain>();
@@ -1672,9 +1737,13 @@ extern "C" int tsk_decode_prepare(tsk_decode_config *config, uint32_t ntasks, in
 extern "C" int tsk_decode_launch(const tsk_decode_task *tasks, uint32_t ntasks,
                                  const tsk_decode_image *images, const tsk_row_start *rows,
                                  tsk_result *results, tsk_decode_config config,
-                                 cudaStream_t stream) {
+                                 uint32_t *claims, cudaStream_t stream) {
     if (ntasks == 0) return cudaSuccess;
     const tsk::Variant v = tsk::select(config.paths, config.shape);
+    if (v.dynamic) {
+        const cudaError_t e = cudaMemsetAsync(claims, 0, sizeof(uint32_t), stream);
+        if (e != cudaSuccess) return e;
+    }
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(config.grid);
     cfg.blockDim = dim3(v.threads);
@@ -1685,7 +1754,8 @@ extern "C" int tsk_decode_launch(const tsk_decode_task *tasks, uint32_t ntasks,
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, v.fn, tasks, ntasks, images, rows, results, 1u, 0x80000000u);
+    return cudaLaunchKernelEx(&cfg, v.fn, tasks, ntasks, images, rows, results, 1u, 0x80000000u,
+                              claims);
 }
 
 // A CUDA graph of one execution: a clear of the result records when the plan has trusted images
@@ -1693,26 +1763,33 @@ extern "C" int tsk_decode_launch(const tsk_decode_task *tasks, uint32_t ntasks,
 extern "C" int tsk_decode_graph(const tsk_decode_task *tasks, uint32_t ntasks,
                                 const tsk_decode_image *images, const tsk_row_start *rows,
                                 tsk_result *results, uint32_t result_count, int clear_results,
-                                tsk_decode_config config, cudaGraph_t *graph_out,
-                                cudaGraphExec_t *exec_out) {
+                                tsk_decode_config config, uint32_t *claims,
+                                cudaGraph_t *graph_out, cudaGraphExec_t *exec_out) {
     cudaGraph_t graph = nullptr;
     cudaError_t e = cudaGraphCreate(&graph, 0);
     if (e != cudaSuccess) return e;
-    cudaGraphNode_t clear = nullptr, kernel = nullptr;
-    if (clear_results && result_count != 0) {
+    const tsk::Variant v = tsk::select(config.paths, config.shape);
+    cudaGraphNode_t before[2] = {nullptr, nullptr}, kernel = nullptr;
+    size_t nbefore = 0;
+    auto clear = [&](void *dst, size_t bytes) {
         cudaMemsetParams m{};
-        m.dst = results;
+        m.dst = dst;
         m.value = 0;
         m.elementSize = 1;
-        m.width = sizeof(tsk_result) * result_count;
+        m.width = bytes;
         m.height = 1;
         m.pitch = 0;
-        e = cudaGraphAddMemsetNode(&clear, graph, nullptr, 0, &m);
+        return cudaGraphAddMemsetNode(&before[nbefore++], graph, nullptr, 0, &m);
+    };
+    if (clear_results && result_count != 0) {
+        e = clear(results, sizeof(tsk_result) * result_count);
+    }
+    if (e == cudaSuccess && v.dynamic && ntasks != 0) {
+        e = clear(claims, sizeof(uint32_t));
     }
     if (e == cudaSuccess && ntasks != 0) {
-        const tsk::Variant v = tsk::select(config.paths, config.shape);
         uint32_t one = 1u, top = 0x80000000u;
-        void *args[] = {&tasks, &ntasks, &images, &rows, &results, &one, &top};
+        void *args[] = {&tasks, &ntasks, &images, &rows, &results, &one, &top, &claims};
         cudaKernelNodeParams k{};
         k.func = reinterpret_cast<void *>(v.fn);
         k.gridDim = dim3(config.grid);
@@ -1720,7 +1797,7 @@ extern "C" int tsk_decode_graph(const tsk_decode_task *tasks, uint32_t ntasks,
         k.sharedMemBytes = static_cast<unsigned>(v.smem);
         k.kernelParams = args;
         k.extra = nullptr;
-        e = cudaGraphAddKernelNode(&kernel, graph, clear ? &clear : nullptr, clear ? 1 : 0, &k);
+        e = cudaGraphAddKernelNode(&kernel, graph, nbefore != 0 ? before : nullptr, nbefore, &k);
     }
     if (e == cudaSuccess) {
         e = cudaGraphInstantiate(exec_out, graph, 0);

@@ -104,7 +104,7 @@ typedef struct {
 // Kernel shapes of the plain uint16 decoder (consumer warps, columns per lane, stages and
 // resident CTAs per SM; listed in decode.cu). Other instances map odd shapes to 0 and even
 // shapes to 2.
-#define TSK_DECODE_SHAPES 18
+#define TSK_DECODE_SHAPES 19
 
 // One image to encode. 96 bytes.
 typedef struct __align__(16) {
@@ -212,19 +212,22 @@ typedef struct {
 
 // --- launchers: return a cudaError_t value (0 = enqueued) ----------------------------------
 
-// Decodes ntasks tasks. results: one record per image. zero_results: the planner has enqueued
-// a clear of the result records (needed by trusted images, whose completion is counted).
+// Decodes ntasks tasks. results: one record per image (the planner clears them first when
+// trusted images count their completion there). claims: 4 bytes of device memory, the work
+// queue's counter, which the launcher clears when the kernel shape uses it (else unused).
 int tsk_decode_launch(const tsk_decode_task *tasks, uint32_t ntasks,
                       const tsk_decode_image *images, const tsk_row_start *rows,
-                      tsk_result *results, tsk_decode_config config, cudaStream_t stream);
+                      tsk_result *results, tsk_decode_config config, uint32_t *claims,
+                      cudaStream_t stream);
 // Occupancy-derived persistent grid for a decode launch, and the kernel preload.
 int tsk_decode_prepare(tsk_decode_config *config, uint32_t ntasks, int device);
-// The same execution as a CUDA graph (clear of the result records when clear_results, then the
-// kernel node), instantiated.
+// The same execution as a CUDA graph (clears of the result records when clear_results and of
+// the work-queue counter when the shape uses it, then the kernel node), instantiated.
 int tsk_decode_graph(const tsk_decode_task *tasks, uint32_t ntasks,
                      const tsk_decode_image *images, const tsk_row_start *rows,
                      tsk_result *results, uint32_t result_count, int clear_results,
-                     tsk_decode_config config, cudaGraph_t *graph, cudaGraphExec_t *exec);
+                     tsk_decode_config config, uint32_t *claims, cudaGraph_t *graph,
+                     cudaGraphExec_t *exec);
 
 // Decodes one serving batch: tile tasks are derived from the requests and the resident archive
 // templates inside the kernel. results: one record per request of the batch. all_u16: every
