@@ -1686,6 +1686,23 @@ def run_profile_case(kind: str, launches: int = 3):
         assert int(res.cpu().numpy().view(np.uint32)[0]) == 0
         print(json.dumps({"profile_case": kind, "launches": launches, "images_per_launch": 1}))
         return
+    if kind == "unparsed":
+        # The headline step's three archives decoded as unparsed files (decode_unparsed_async:
+        # index entries, payloads and rows validated on the device), one launch each time.
+        frame, shapes, step_plans, workspace, results = prepare_workload(torch, stream, 1)
+        entries = [(ConstBytes(s["copies"][0]["src"].data_ptr(), len(s["file"])), s["file"][:64],
+                    api.view(s["copies"][0]["out"], 1, W, H, W * 2)) for s in shapes]
+        for _ in range(launches):
+            assert cuda.decode_unparsed_async(entries, api.ResultBuffer(results.data_ptr(), 3),
+                                              stream) == Status.success
+        torch.cuda.synchronize()
+        recs = results.cpu().numpy().view(np.uint64).reshape(-1, 2)[:3]
+        assert all(int(r[0]) == 0 for r in recs), recs
+        for s in shapes:
+            assert np.array_equal(s["copies"][0]["out"].cpu().numpy().view(np.uint16),
+                                  frame.reshape(-1))
+        print(json.dumps({"profile_case": kind, "launches": launches, "images_per_launch": 3}))
+        return
     if kind == "step":
         frame, shapes, step_plans, workspace, results = prepare_workload(torch, stream, 1)
         wsb = api.MutableBytes(workspace.data_ptr(), workspace.numel())
@@ -1754,7 +1771,7 @@ def run_profile_case(kind: str, launches: int = 3):
 def main():
     p = argparse.ArgumentParser()
     p.add_argument("--profile", choices=["decode", "fused", "encode", "step", "field",
-                                         "calibrate", "batch", "serve", "stage"],
+                                         "calibrate", "batch", "serve", "stage", "unparsed"],
                    default=None,
                    help="run only a small case for ncu captures and exit")
     p.add_argument("--gpus", type=int, default=1)

@@ -826,6 +826,7 @@ __device__ __forceinline__ tsk_decode_task load_task(const tsk_decode_task *p) {
 // TableSource: a planned queue of tasks and its image table (every plan and mixed batch).
 struct TableSource {
     static constexpr bool kTrusted = true;
+    static constexpr bool kLocalCounts = false;
     const tsk_decode_task *tasks;
     const tsk_decode_image *images;
     uint32_t ntasks;
@@ -861,6 +862,7 @@ struct TableSource {
 // (plan.cpp clip(), after reference plan.cpp:281-349), so no task table is uploaded.
 struct ServeSource {
     static constexpr bool kTrusted = false;
+    static constexpr bool kLocalCounts = false;
     const tsk_serve_batch *batch;
     const tsk_serve_archive *archives;
     uint32_t ntasks;
@@ -931,9 +933,30 @@ struct ServeSource {
 // it as malformed data.
 struct FileSource {
     static constexpr bool kTrusted = true;
+    static constexpr bool kLocalCounts = true;
     const tsk_file_batch *batch;
     uint32_t ntasks;
     uint32_t cursor; // file of the last task asked for (indexes only increase)
+    uint32_t *done;  // shared memory: this CTA's finished tiles per file
+
+    // Adds this CTA's finished tiles of file k to its record's count; the CTA that completes
+    // the count writes the final record (the failures CAS-ed before are visible to it).
+    __device__ void flush(uint32_t k, tsk_result *results) const {
+        const uint32_t c = done[k];
+        if (c == 0) {
+            return;
+        }
+        const tsk_decode_image &im = batch->files[k].image;
+        __threadfence();
+        const uint32_t before = atomicAdd(&results[k].reserved, c);
+        if (before + c == im.tile_count) {
+            __threadfence();
+            const uint32_t status = *reinterpret_cast<volatile uint32_t *>(&results[k].status);
+            results[k].reserved = 0;
+            results[k].bytes_written = status == 0 ? im.result_bytes : 0;
+            results[k].status = status;
+        }
+    }
 
     __device__ tsk_decode_task task(uint32_t g) {
         const tsk_file *files = batch->files;
@@ -946,6 +969,10 @@ struct FileSource {
         const uint32_t trow = l / f.tiles_across, tcol = l % f.tiles_across;
         const uint64_t x = static_cast<uint64_t>(tcol) * im.tile_width;
         const uint64_t y = static_cast<uint64_t>(trow) * im.tile_height;
+        // The producer asks for a task one tile ahead: its index entry (and the previous one,
+        // for the payload chain) is on its way to L2 when the tile is staged.
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(f.src + 32 + 32ull * l));
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(f.src + 64 + 32ull * l));
         tsk_decode_task t{};
         t.src = f.src;
         t.words_or_tile = l;
@@ -1206,10 +1233,16 @@ __device__ __forceinline__ void consume_tile(Sh &sh, uint32_t s, const Source &s
                 if (state == kStageMalformed || (state == kStageOk && !ok)) {
                     fail(results, t.image, 5u); // malformed_data
                 }
-                // Completion count: the last task of the image writes the final record.
-                __threadfence();
-                const uint32_t done = atomicAdd(&results[t.image].reserved, 1u);
-                if (done + 1 == im.tile_count) {
+                // Completion count: the last task of the image writes the final record. A
+                // source with per-CTA tallies (FileSource) adds them once per CTA instead.
+                uint32_t done = 0;
+                if constexpr (Source::kLocalCounts) {
+                    atomicAdd(&source.done[t.image], 1u);
+                } else {
+                    __threadfence();
+                    done = atomicAdd(&results[t.image].reserved, 1u) + 1;
+                }
+                if (!Source::kLocalCounts && done == im.tile_count) {
                     __threadfence();
                     uint32_t status =
                         *reinterpret_cast<volatile uint32_t *>(&results[t.image].status);
@@ -1368,16 +1401,24 @@ __device__ __forceinline__ void decode_body(Source &source, const tsk_row_start 
                 fail(results, Dyn ? last_image : source.image_of(blockIdx.x + i * gridDim.x),
                      9u); // cuda_error
             }
-            return;
+            break;
         }
         if constexpr (Dyn) {
             if (sh.header[s].state == kStageEnd) {
-                return;
+                break;
             }
             last_image = sh.header[s].task.image;
         }
         consume_tile<Paths, RW, G16, NR, true>(sh, s, source, results, one, top, lead, slot,
                                                group);
+    }
+    if constexpr (Source::kLocalCounts) {
+        // Every consumer warp is past its last tile (or gave up on a stage): the CTA's tallies
+        // are final. Barrier 15 is used by nothing else.
+        named_sync(15, kConsumers);
+        if (threadIdx.x < source.batch->count) {
+            source.flush(threadIdx.x, results);
+        }
     }
 }
 
@@ -1501,7 +1542,11 @@ template <uint32_t MaxPayload, uint32_t Stages, uint32_t Paths, uint32_t CW, uin
 __global__ void __launch_bounds__(threads_of(CW), MinBlocks)
     file_kernel(const __grid_constant__ tsk_file_batch batch, tsk_result *results, uint32_t one,
                 uint32_t top) {
-    FileSource source{&batch, batch.ntasks, 0};
+    __shared__ uint32_t done[TSK_FILE_MAX_BATCH];
+    if (threadIdx.x < TSK_FILE_MAX_BATCH) {
+        done[threadIdx.x] = 0; // ordered before use by decode_body's first __syncthreads
+    }
+    FileSource source{&batch, batch.ntasks, 0, done};
     decode_body<MaxPayload, Stages, Paths, CW, G16, NR, RW>(source, nullptr, results, one, top);
 }
 
