@@ -1123,20 +1123,15 @@ Status autotune(detail::PlanState &p, tsk_result *results, const char *cache, cu
     std::lock_guard<std::mutex> lock(g_tune_mutex);
     load_tune_cache(cache);
     const std::string key = tune_key(p, p.device);
-    int sms = 0;
-    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p.device) != cudaSuccess) {
-        return detail::cuda_failure("cudaDeviceGetAttribute");
-    }
     auto apply = [&](std::uint32_t shape, std::uint32_t per_sm) -> cudaError_t {
         tsk_decode_config c = p.config;
         c.shape = shape;
-        const int e = tsk_decode_prepare(&c, p.task_count, p.device);
+        int e = tsk_decode_prepare(&c, p.task_count, p.device);
+        if (e == 0 && per_sm != 0 && per_sm != c.per_sm) {
+            // Fewer (or, up to the occupancy, more) resident CTAs than the shape's default.
+            e = tsk_decode_residency(&c, per_sm, p.task_count, p.device);
+        }
         if (e != 0) return static_cast<cudaError_t>(e);
-        const std::uint32_t k = per_sm == 0 || per_sm > c.per_sm ? c.per_sm : per_sm;
-        const std::uint64_t grid = static_cast<std::uint64_t>(sms) * k;
-        c.grid = static_cast<std::uint32_t>(std::max<std::uint64_t>(
-            1, std::min<std::uint64_t>(grid, p.task_count)));
-        c.per_sm = k;
         p.config = c;
         return cudaSuccess;
     };
@@ -1166,7 +1161,7 @@ Status autotune(detail::PlanState &p, tsk_result *results, const char *cache, cu
         tsk_decode_config probe = p.config;
         probe.shape = shapes[i];
         e = static_cast<cudaError_t>(tsk_decode_prepare(&probe, p.task_count, p.device));
-        for (std::uint32_t k = probe.per_sm; k >= 1 && e == cudaSuccess; --k) {
+        for (std::uint32_t k = probe.fits; k >= 1 && e == cudaSuccess; --k) {
             e = apply(shapes[i], k);
             if (e == cudaSuccess) e = enqueue_decode(p, results, stream); // warm-up
             constexpr int kRuns = 3;
@@ -1183,7 +1178,7 @@ Status autotune(detail::PlanState &p, tsk_result *results, const char *cache, cu
                 best_us = us;
                 best = {shapes[i], k};
             }
-            if (k + 2 < probe.per_sm) {
+            if (k + 2 < probe.fits) {
                 break; // fewer CTAs than that never won on this kernel
             }
         }

@@ -1140,8 +1140,8 @@ __device__ void stage_task(Sh &sh, uint32_t s, const tsk_decode_task &t, const S
 // warp's index in it), then writes the tile's result-record updates (lead thread). Release: the
 // stage is handed back through its empty barrier (producer-warp mode); self-staging groups
 // reuse their stages themselves.
-template <uint32_t Paths, uint32_t RW, uint32_t G16, uint32_t NR, bool Release, typename Sh,
-          typename Source>
+template <uint32_t Paths, uint32_t RW, uint32_t G16, uint32_t NR, bool Release, uint32_t Groups,
+          typename Sh, typename Source>
 __device__ __forceinline__ void consume_tile(Sh &sh, uint32_t s, const Source &source,
                                              tsk_result *results, uint32_t one, uint32_t top,
                                              bool lead, uint32_t slot, uint32_t group) {
@@ -1173,7 +1173,7 @@ __device__ __forceinline__ void consume_tile(Sh &sh, uint32_t s, const Source &s
         if constexpr (RW == 1) {
             __syncwarp();
         } else {
-            named_sync(1 + group, RW * 32);
+            group_sync<Groups>(group, RW * 32);
         }
         ok = sh.valid[s] != 0;
     }
@@ -1279,7 +1279,7 @@ __device__ __forceinline__ void consume_tile(Sh &sh, uint32_t s, const Source &s
 // ahead, so CTAs that drew cheap tiles take more of them; after the last task it stages one end
 // marker per consumer group.
 template <uint32_t MaxPayload, uint32_t Stages, uint32_t Paths, uint32_t CW, uint32_t G16,
-          uint32_t NR, uint32_t RW, bool Dyn = false, typename Source>
+          uint32_t NR, uint32_t RW, bool Dyn = false, bool Reserve = false, typename Source>
 __device__ __forceinline__ void decode_body(Source &source, const tsk_row_start *rowtab,
                                             tsk_result *results, uint32_t one, uint32_t top) {
     using Sh = Shared<MaxPayload, Stages>;
@@ -1409,13 +1409,14 @@ __device__ __forceinline__ void decode_body(Source &source, const tsk_row_start 
             }
             last_image = sh.header[s].task.image;
         }
-        consume_tile<Paths, RW, G16, NR, true>(sh, s, source, results, one, top, lead, slot,
+        consume_tile<Paths, RW, G16, NR, true, Reserve ? 0u : kGroups>(sh, s, source, results, one,
+                                                                        top, lead, slot,
                                                group);
     }
     if constexpr (Source::kLocalCounts) {
         // Every consumer warp is past its last tile (or gave up on a stage): the CTA's tallies
-        // are final. Barrier 15 is used by nothing else.
-        named_sync(15, kConsumers);
+        // are final. Barrier 1 + kGroups is used by nothing else.
+        named_sync<1 + kGroups>(kConsumers);
         if (threadIdx.x < source.batch->count) {
             source.flush(threadIdx.x, results);
         }
@@ -1457,11 +1458,11 @@ __device__ __forceinline__ void decode_body_self(Source &source, const tsk_row_s
     // This group's k-th tile is the CTA's tile group + k * kGroups.
     const uint32_t count = group < mine ? (mine - 1 - group) / kGroups + 1 : 0;
     auto queue_index = [&](uint32_t k) { return blockIdx.x + (group + k * kGroups) * gridDim.x; };
-    auto group_sync = [&]() {
+    auto sync_group = [&]() {
         if constexpr (RW == 1) {
             __syncwarp();
         } else {
-            named_sync(1 + group, RW * 32);
+            tsk::group_sync<kGroups>(group, RW * 32);
         }
     };
     // Task records and parsed payloads are staged before waiting for the stream's previous
@@ -1491,10 +1492,10 @@ __device__ __forceinline__ void decode_body_self(Source &source, const tsk_row_s
             }
             return;
         }
-        consume_tile<Paths, RW, G16, NR, false>(sh, s, source, results, one, top, lead, slot,
+        consume_tile<Paths, RW, G16, NR, false, kGroups>(sh, s, source, results, one, top, lead, slot,
                                                 group);
         if (k + 2 < count) {
-            group_sync(); // every warp of the group is done with stage s
+            sync_group(); // every warp of the group is done with stage s
             if (lead) {
                 const tsk_decode_task t = next;
                 if (k + 3 < count) {
@@ -1507,8 +1508,11 @@ __device__ __forceinline__ void decode_body_self(Source &source, const tsk_row_s
 }
 
 // A planned queue (every plan and mixed batch); MinBlocks resident CTAs per SM.
+// Reserve: the kernel reserves all sixteen named barriers (named_sync_any), which holds an SM
+// to four resident CTAs; the default uint16 shape measured fastest so (faster than with five,
+// and than four enforced by padded shared memory).
 template <uint32_t MaxPayload, uint32_t Stages, uint32_t Paths, uint32_t CW, uint32_t G16,
-          uint32_t MinBlocks, uint32_t NR, uint32_t RW, bool Self, bool Dyn>
+          uint32_t MinBlocks, uint32_t NR, uint32_t RW, bool Self, bool Dyn, bool Reserve>
 __global__ void __launch_bounds__(threads_of(CW, Self), MinBlocks)
     decode_kernel(const tsk_decode_task *__restrict__ tasks, uint32_t ntasks,
                   const tsk_decode_image *__restrict__ images,
@@ -1519,8 +1523,8 @@ __global__ void __launch_bounds__(threads_of(CW, Self), MinBlocks)
         decode_body_self<MaxPayload, Stages, Paths, CW, G16, NR, RW>(source, rowtab, results, one,
                                                                       top);
     } else {
-        decode_body<MaxPayload, Stages, Paths, CW, G16, NR, RW, Dyn>(source, rowtab, results,
-                                                                      one, top);
+        decode_body<MaxPayload, Stages, Paths, CW, G16, NR, RW, Dyn, Reserve>(source, rowtab,
+                                                                               results, one, top);
     }
 }
 
@@ -1566,19 +1570,23 @@ struct Variant {
 // headline one, comes in four shapes (consumer warps x columns per lane) for the tuner.
 template <uint32_t MaxPayload, uint32_t Stages, uint32_t Paths, uint32_t CW = 8,
           uint32_t G16 = 8, uint32_t MinBlocks = 3, uint32_t NR = 0, uint32_t RW = CW,
-          bool Self = false, bool Dyn = false>
+          bool Self = false, bool Dyn = false, bool Reserve = false>
 Variant make() {
-    return {decode_kernel<MaxPayload, Stages, Paths, CW, G16, MinBlocks, NR, RW, Self, Dyn>,
+    return {decode_kernel<MaxPayload, Stages, Paths, CW, G16, MinBlocks, NR, RW, Self, Dyn, Reserve>,
             sizeof(Shared<MaxPayload, Stages>), threads_of(CW, Self), Dyn};
 }
 
 // Shapes of the plain uint16 instance (consumer warps x uint16 columns per lane, stages,
-// resident CTAs per SM): 0 = 8 x 8, 4 stages, 4; 1 = 8 x 16, 4, 3; 2 = 4 x 16, 4, 5;
-// 3 = 4 x 8, 4, 6; 4 = 4 x 16, 4, 6 (64 registers); 5 = 4 x 16, 3, 7 (56 registers);
-// 6 = 4 x 32, 4, 3; 7 = 4 x 32, 4, 4. The plain mixed uint16 + FP32 instance has four: 0 =
-// 8 x 8, 3 stages of 16 KiB, 3 CTAs; 1 = 4 x 16, 2 stages, 5 CTAs; 2 = 4 x 16, 3, 4; 3 = 4 x 8,
-// 2, 6 (two stages leave shared memory for more resident CTAs). The other instances have shapes
-// 0 and 2 (odd shapes map to 0, even ones to 2).
+// resident CTAs per SM in the launch bounds): 0 = 8 x 8, 4 stages, 4; 1 = 8 x 16, 4, 3;
+// 2 = 4 x 16, 4, 5; 3 = 4 x 8, 4, 6; 4 = 4 x 16, 4, 6 (64 registers); 5 = 4 x 16, 3, 7 (56
+// registers); 6 = 4 x 32, 4, 3; 7 = 4 x 32, 4, 4; 8-11 single-pass rows with one or two rows per
+// lane; 12-13 warps in groups of one or two per tile (13, the default: pairs, four CTAs per
+// SM); 14-17 without a producer warp (each group stages its own tiles); 18 = 13 with
+// the device work queue. The plain mixed uint16 + FP32 instance has ten: 0 = 8 x 8, 3 stages of
+// 16 KiB, 3 CTAs; 1 = 4 x 16, 2 stages, 5 CTAs; 2 = 4 x 16, 3, 4; 3 = 4 x 8, 2, 6 (two stages
+// leave shared memory for more resident CTAs); 4-7 variants of them with single-pass rows or
+// warp pairs; 8 and 9 = 5 and 6 with the device work queue. The other instances have shapes 0
+// and 2 (odd shapes map to 0, even ones to 2), and single-pass rows from shape 8 on.
 Variant select(uint32_t paths, uint32_t shape) {
     const bool f32 = paths & kF32, u16 = paths & kU16, plain = paths & kPlain, c = paths & kCal;
     const bool narrow = shape % 2 == 0 && shape != 0; // four consumer warps
@@ -1609,8 +1617,8 @@ Variant select(uint32_t paths, uint32_t shape) {
                 return make<8192, 4, kU16 | kPlain, 4, 8, 5, 2>();
             case 12:
                 return make<8192, 5, kU16 | kPlain, 4, 16, 4, 1, 1>();
-            case 13:
-                return make<8192, 4, kU16 | kPlain, 4, 16, 5, 1, 2>();
+            case 13: // four CTAs per SM (all named barriers reserved)
+                return make<8192, 4, kU16 | kPlain, 4, 16, 5, 1, 2, false, false, true>();
             case 14:
                 return make<8192, 4, kU16 | kPlain, 4, 16, 5, 1, 2, true>();
             case 15:
@@ -1734,6 +1742,42 @@ int g_prepared_count = 0;
 
 } // namespace
 
+// Dynamic shared memory per CTA with which exactly per_sm CTAs of v share an SM when its
+// occupancy (`fits` CTAs) is higher: the block scheduler places as many CTAs on an SM as fit,
+// so a grid of SMs x per_sm CTAs would otherwise leave SMs empty. Never below v's own need.
+size_t residency_smem(const tsk::Variant &v, int per_sm, int fits, int device) {
+    if (per_sm >= fits) {
+        return v.smem;
+    }
+    int total = 0, reserved = 0;
+    if (cudaDeviceGetAttribute(&total, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device) !=
+            cudaSuccess ||
+        cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, device) !=
+            cudaSuccess) {
+        cudaGetLastError();
+        return v.smem;
+    }
+    // (per_sm + 1) CTAs of this size exceed the SM's shared memory; per_sm still fit.
+    const size_t padded = static_cast<size_t>(total / (per_sm + 1) - reserved + 1 + 127) / 128 * 128;
+    const size_t smem = padded > v.smem ? padded : v.smem;
+    return static_cast<size_t>(per_sm) * (smem + reserved) <= static_cast<size_t>(total) ? smem
+                                                                                         : v.smem;
+}
+
+// The grid and shared memory of a launch for per_sm resident CTAs per SM (at most the
+// occupancy of the instance, `fits`).
+void set_residency(tsk_decode_config *config, const tsk::Variant &v, int per_sm, int fits,
+                   int sms, uint32_t ntasks, int device) {
+    if (per_sm > fits) per_sm = fits;
+    if (per_sm < 1) per_sm = 1;
+    uint64_t grid = static_cast<uint64_t>(sms) * per_sm;
+    if (grid > ntasks) grid = ntasks;
+    if (grid < 1) grid = 1;
+    config->grid = static_cast<uint32_t>(grid);
+    config->per_sm = static_cast<uint32_t>(per_sm);
+    config->smem = static_cast<uint32_t>(residency_smem(v, per_sm, fits, device));
+}
+
 extern "C" int tsk_decode_prepare(tsk_decode_config *config, uint32_t ntasks, int device) {
     const tsk::Variant v = tsk::select(config->paths, config->shape);
     const void *key = reinterpret_cast<const void *>(v.fn);
@@ -1748,8 +1792,12 @@ extern "C" int tsk_decode_prepare(tsk_decode_config *config, uint32_t ntasks, in
             }
         }
     }
-    cudaError_t e = cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(v.smem));
+    // Any padding set_residency chooses is allowed: the limit is the device's per-block maximum.
+    int optin = 0;
+    cudaError_t e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             optin > static_cast<int>(v.smem) ? optin : static_cast<int>(v.smem));
     if (e != cudaSuccess) return e;
     // The largest shared-memory carveout, so that occupancy is bounded by the instance's own
     // needs and not by the default split between L1 and shared memory.
@@ -1766,13 +1814,20 @@ extern "C" int tsk_decode_prepare(tsk_decode_config *config, uint32_t ntasks, in
             g_prepared[g_prepared_count++] = {device, key, per_sm, sms};
         }
     }
-    if (per_sm < 1) per_sm = 1;
-    uint64_t grid = static_cast<uint64_t>(sms) * per_sm;
-    if (grid > ntasks) grid = ntasks;
-    if (grid < 1) grid = 1;
-    config->grid = static_cast<uint32_t>(grid);
-    config->per_sm = static_cast<uint32_t>(per_sm);
-    config->smem = static_cast<uint32_t>(v.smem);
+    const int fits = per_sm < 1 ? 1 : per_sm;
+    set_residency(config, v, fits, fits, sms, ntasks, device);
+    config->fits = static_cast<uint32_t>(fits);
+    return cudaSuccess;
+}
+
+extern "C" int tsk_decode_residency(tsk_decode_config *config, uint32_t per_sm, uint32_t ntasks,
+                                    int device) {
+    const tsk::Variant v = tsk::select(config->paths, config->shape);
+    int sms = 0;
+    const cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (e != cudaSuccess) return e;
+    set_residency(config, v, static_cast<int>(per_sm), static_cast<int>(config->fits), sms, ntasks,
+                  device);
     return cudaSuccess;
 }
 
@@ -1792,7 +1847,7 @@ extern "C" int tsk_decode_launch(const tsk_decode_task *tasks, uint32_t ntasks,
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(config.grid);
     cfg.blockDim = dim3(v.threads);
-    cfg.dynamicSmemBytes = v.smem;
+    cfg.dynamicSmemBytes = config.smem;
     cfg.stream = stream;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -1839,7 +1894,7 @@ extern "C" int tsk_decode_graph(const tsk_decode_task *tasks, uint32_t ntasks,
         k.func = reinterpret_cast<void *>(v.fn);
         k.gridDim = dim3(config.grid);
         k.blockDim = dim3(v.threads);
-        k.sharedMemBytes = static_cast<unsigned>(v.smem);
+        k.sharedMemBytes = config.smem;
         k.kernelParams = args;
         k.extra = nullptr;
         e = cudaGraphAddKernelNode(&kernel, graph, nbefore != 0 ? before : nullptr, nbefore, &k);

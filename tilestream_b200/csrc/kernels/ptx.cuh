@@ -129,9 +129,39 @@ __device__ __forceinline__ void griddep_launch_dependents() {
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
-// Named barrier over a subset of the CTA's warps.
-__device__ __forceinline__ void named_sync(uint32_t id, uint32_t threads) {
+// Named barrier over a subset of the CTA's warps. The id is an immediate: a barrier id known
+// only at run time makes the compiler reserve all sixteen barriers for the kernel, and the
+// barriers a CTA reserves bound how many CTAs an SM holds.
+template <uint32_t Id> __device__ __forceinline__ void named_sync(uint32_t threads) {
+    static_assert(Id < 16, "sixteen hardware barriers");
+    asm volatile("bar.sync %0, %1;" ::"n"(Id), "r"(threads) : "memory");
+}
+
+// The same with the id in a register: the kernel then reserves all sixteen barriers, which
+// limits an SM to four CTAs (64 barriers per SM). Used where that limit is the intent.
+__device__ __forceinline__ void named_sync_any(uint32_t id, uint32_t threads) {
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(threads) : "memory");
+}
+
+// Barrier 1 + group for one of Groups groups of warps (barriers 1 .. Groups). Groups = 0: the
+// id in a register (named_sync_any).
+template <uint32_t Groups>
+__device__ __forceinline__ void group_sync(uint32_t group, uint32_t threads) {
+    static_assert(Groups <= 8, "at most eight groups");
+    if constexpr (Groups == 0) {
+        named_sync_any(1 + group, threads);
+        return;
+    }
+    switch (group) {
+    case 0: named_sync<1>(threads); break;
+    case 1: if constexpr (Groups > 1) named_sync<2>(threads); break;
+    case 2: if constexpr (Groups > 2) named_sync<3>(threads); break;
+    case 3: if constexpr (Groups > 3) named_sync<4>(threads); break;
+    case 4: if constexpr (Groups > 4) named_sync<5>(threads); break;
+    case 5: if constexpr (Groups > 5) named_sync<6>(threads); break;
+    case 6: if constexpr (Groups > 6) named_sync<7>(threads); break;
+    default: if constexpr (Groups > 7) named_sync<8>(threads); break;
+    }
 }
 
 // 16-byte store to global memory (an evict-first hint measured slower). No memory clobber: the

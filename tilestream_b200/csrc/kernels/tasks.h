@@ -94,11 +94,12 @@ enum {
 // Launch parameters of a decode plan: `paths` is set by the planner, the rest by
 // tsk_decode_prepare (and may be lowered by the autotuner).
 typedef struct {
-    uint32_t grid;   // persistent CTAs
-    uint32_t per_sm; // resident CTAs per SM at the kernel's occupancy
-    uint32_t smem;   // dynamic shared memory per CTA in bytes
+    uint32_t grid;   // persistent CTAs: SMs x per_sm (at most the task count)
+    uint32_t per_sm; // resident CTAs per SM the launch is sized for
+    uint32_t smem;   // dynamic shared memory per CTA in bytes (padded so that per_sm fit exactly)
     uint32_t paths;  // TSK_PATH_* mask selecting the kernel instance
     uint32_t shape;  // plain uint16 kernel shape, 0 .. TSK_DECODE_SHAPES - 1 (decode.cu)
+    uint32_t fits;   // resident CTAs per SM at the instance's occupancy
 } tsk_decode_config;
 
 // Kernel shapes of the plain uint16 decoder (consumer warps, columns per lane, stages and
@@ -221,6 +222,9 @@ int tsk_decode_launch(const tsk_decode_task *tasks, uint32_t ntasks,
                       cudaStream_t stream);
 // Occupancy-derived persistent grid for a decode launch, and the kernel preload.
 int tsk_decode_prepare(tsk_decode_config *config, uint32_t ntasks, int device);
+// Re-sizes a prepared launch for per_sm resident CTAs per SM (at most config->fits): the grid,
+// and shared memory padded so that no more CTAs share an SM.
+int tsk_decode_residency(tsk_decode_config *config, uint32_t per_sm, uint32_t ntasks, int device);
 // The same execution as a CUDA graph (clears of the result records when clear_results and of
 // the work-queue counter when the shape uses it, then the kernel node), instantiated.
 int tsk_decode_graph(const tsk_decode_task *tasks, uint32_t ntasks,
