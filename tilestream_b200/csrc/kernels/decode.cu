@@ -77,7 +77,8 @@ template <uint32_t MaxPayload, uint32_t Stages> struct Shared {
     alignas(16) StageHeader header[Stages];
     alignas(8) uint64_t full[Stages];
     alignas(8) uint64_t empty[Stages];
-    uint32_t valid[Stages]; // trusted row walk verdict of the staged tile
+    uint32_t valid[Stages];   // trusted row walk verdict of the staged tile
+    uint32_t rowfail[Stages]; // set when a row check of the group's threads fails
 };
 
 // Paths compiled into one kernel instance.
@@ -770,37 +771,51 @@ __device__ __forceinline__ void decode_tile(const Ctx &x, const uint32_t *payloa
     }
 }
 
-// Reads the row descriptors of an encoder-produced tile (decoder.cu:86-110): false when they do
-// not describe exactly the staged payload. The width word is compared whole, so its three
-// reserved bytes must be zero. strict (unparsed files) adds the host parser's remaining row
-// rules (parser.cpp check_payloads, after reference src/cpu/parser.cpp:127-171): a one-column
-// tile has zero-width rows, and the unused high bits of a row's last packed word are zero.
-__device__ bool walk_rows(const uint32_t *payload, uint32_t words, uint32_t width,
-                          uint32_t height, bool f32, uint16_t *rows, bool strict) {
-    const uint32_t max_bits = f32 ? 32u : 16u;
+// Locates the row descriptors of a tile whose rows are read on the device (encoder output,
+// reference decoder.cu:86-110, and unparsed files): the serial part of the row walk, one lane.
+// Each row starts where the previous one's packed words end; a width word above the widest
+// sample (which also catches nonzero reserved bytes, as the word is compared whole) or a row
+// that does not fit ends the walk. False unless the rows end exactly at the payload's end.
+// The per-row checks that need no chain run on every thread of the group (row_ok).
+__device__ bool chain_rows(const uint32_t *payload, uint32_t words, uint32_t width,
+                           uint32_t height, bool f32, uint16_t *rows) {
+    const uint32_t max_bits = f32 ? 32u : 16u, wm1 = width - 1;
     uint32_t cursor = 0;
     for (uint32_t r = 0; r < height; ++r) {
         if (words - cursor < 2) {
             return false;
         }
-        const uint32_t seed = payload[cursor];
         const uint32_t bits = payload[cursor + 1];
-        if (bits > max_bits || (!f32 && seed > 65535u)) {
-            return false;
-        }
-        const uint32_t nbits = (width - 1) * bits;
-        const uint32_t packed = (nbits + 31) / 32;
-        if (words - cursor - 2 < packed) {
-            return false;
-        }
-        if (strict && ((width == 1 && bits != 0) ||
-                       (nbits % 32 != 0 && (payload[cursor + 1 + packed] >> (nbits % 32)) != 0))) {
+        if (bits > max_bits) {
             return false;
         }
         rows[r] = static_cast<uint16_t>(cursor);
-        cursor += 2 + packed;
+        cursor += 2 + ((wm1 * bits + 31) >> 5);
+        if (cursor > words) {
+            return false;
+        }
     }
     return cursor == words;
+}
+
+// The checks of one located row: the seed of a uint16 row is a uint16 value; strict (unparsed
+// files) adds the host parser's remaining row rules (parser.cpp check_payloads, after reference
+// src/cpu/parser.cpp:127-171): a one-column tile has zero-width rows, and the unused high bits
+// of the row's last packed word are zero.
+__device__ __forceinline__ bool row_ok(const uint32_t *payload, uint32_t start, uint32_t width,
+                                       bool f32, bool strict) {
+    const uint32_t seed = payload[start], bits = payload[start + 1];
+    if (!f32 && seed > 65535u) {
+        return false;
+    }
+    if (strict) {
+        const uint32_t nbits = (width - 1) * bits, packed = (nbits + 31) / 32;
+        if ((width == 1 && bits != 0) ||
+            (nbits % 32 != 0 && (payload[start + 1 + packed] >> (nbits % 32)) != 0)) {
+            return false;
+        }
+    }
+    return true;
 }
 
 __device__ __forceinline__ void fail(tsk_result *results, uint32_t image, uint32_t status) {
@@ -1156,10 +1171,17 @@ __device__ __forceinline__ void consume_tile(Sh &sh, uint32_t s, const Source &s
     const bool unparsed = (t.flags & TSK_UNPARSED) != 0;
     bool ok = state == kStageOk;
     if (trusted && ok && (hmode == TSK_PREDICT || unparsed)) {
+        auto sync = [&]() {
+            if constexpr (RW == 1) {
+                __syncwarp();
+            } else {
+                group_sync<Groups>(group, RW * 32);
+            }
+        };
         if (lead) {
             bool valid;
             if (hmode == TSK_PREDICT) {
-                valid = walk_rows(payload, h.words, t.width, t.height, f32, sh.rows[s], unparsed);
+                valid = chain_rows(payload, h.words, t.width, t.height, f32, sh.rows[s]);
             } else if (hmode == TSK_RAW) {
                 // The bytes after the last sample are zero.
                 const uint32_t tail = (static_cast<uint32_t>(t.width) * t.height * 2u) % 4u;
@@ -1169,13 +1191,20 @@ __device__ __forceinline__ void consume_tile(Sh &sh, uint32_t s, const Source &s
                 valid = f32 || (payload[0] >> 16) == 0;
             }
             sh.valid[s] = valid;
+            sh.rowfail[s] = 0;
         }
-        if constexpr (RW == 1) {
-            __syncwarp();
-        } else {
-            group_sync<Groups>(group, RW * 32);
+        sync();
+        ok = sh.valid[s] != 0; // read by every thread before any writes rowfail
+        if (ok && hmode == TSK_PREDICT) {
+            // The rows' own checks, one row per thread of the group.
+            for (uint32_t r = slot * 32 + lane; r < t.height; r += RW * 32) {
+                if (!row_ok(payload, sh.rows[s][r], t.width, f32, unparsed)) {
+                    sh.rowfail[s] = 1;
+                }
+            }
+            sync();
+            ok = sh.rowfail[s] == 0;
         }
-        ok = sh.valid[s] != 0;
     }
     if (ok) {
         Ctx x;
