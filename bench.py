@@ -433,7 +433,10 @@ def run_ours(args, rank, world, device, torch, dist):
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                      "peak_source": peak_src, "unit": "GB/s", "frac": round(achieved / peak, 4),
                      "algorithmic_bytes_per_launch": int(alg_per_launch),
-                     "traffic": ncu_traffic(), "kernel": "decode_kernel"},
+                     "traffic": ncu_traffic(),
+                     "traffic_source": "copied from the committed ncu capture of the same launch "
+                                       "(profiles/decode_step_3_archives.md), not measured here",
+                     "kernel": "decode_kernel"},
         "e2e": e2e,
         "clocks": clocks.report(),
     }
