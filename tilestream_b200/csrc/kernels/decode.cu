@@ -777,21 +777,20 @@ __device__ __forceinline__ void decode_tile(const Ctx &x, const uint32_t *payloa
 // sample (which also catches nonzero reserved bytes, as the word is compared whole) or a row
 // that does not fit ends the walk. False unless the rows end exactly at the payload's end.
 // The per-row checks that need no chain run on every thread of the group (row_ok).
+//
+// The loop carries as little as it can: the width word of a row that starts past the payload's
+// end is read from the stage's slack (the stage holds a whole tile plus slack, and the walk
+// stops as soon as a row ends past the payload, so it reads at most one word beyond it), and
+// the row is then rejected by the end check, which covers the descriptor's own two words.
 __device__ bool chain_rows(const uint32_t *payload, uint32_t words, uint32_t width,
                            uint32_t height, bool f32, uint16_t *rows) {
     const uint32_t max_bits = f32 ? 32u : 16u, wm1 = width - 1;
     uint32_t cursor = 0;
     for (uint32_t r = 0; r < height; ++r) {
-        if (words - cursor < 2) {
-            return false;
-        }
         const uint32_t bits = payload[cursor + 1];
-        if (bits > max_bits) {
-            return false;
-        }
         rows[r] = static_cast<uint16_t>(cursor);
-        cursor += 2 + ((wm1 * bits + 31) >> 5);
-        if (cursor > words) {
+        cursor += 2 + ((wm1 * (bits <= max_bits ? bits : 0u) + 31) >> 5);
+        if (bits > max_bits || cursor > words) {
             return false;
         }
     }
