@@ -1025,7 +1025,10 @@ def run_archive_roi(args, torch, shapes):
     Three ways to get the payloads to the device are timed: `direct` (stage_roi_tiles: one copy
     per tile row straight from the pinned archive), `gather` (the reference's way: host copies
     of the ROI's tiles into a pinned staging buffer, then one copy) and `whole_archive` (the
-    whole file copied per request). Decoded bytes count ROI pixels at 2 B (the stored type)."""
+    whole file copied per request). `direct_batched` stages the same way but decodes the 64
+    requests as one mixed batch (one plan and one launch for all of them: throughput, with the
+    batch's latency for every request). Decoded bytes count ROI pixels at 2 B (the stored
+    type)."""
     from tilestream_b200 import api, cuda
     from tilestream_b200.api import (BatchItem, Calibration, CompressedInput, ConstBytes,
                                      MutableBytes, Roi, Status, TileMapping)
@@ -1112,7 +1115,30 @@ def run_archive_roi(args, torch, shapes):
 
     host_us = {"stage": 0.0, "prepare": 0.0, "launch": 0.0}
 
+    def step_batched():
+        """All the batch's ROIs staged on the copy stream, then one mixed batch of their 64
+        decode_calibrate items (one plan, one launch) after the copies' event."""
+        for i, (a, roi) in enumerate(reqs):
+            s = slots[i]
+            st, _ = cuda.stage_roi_tiles(
+                shapes[a]["meta"], Roi(*roi), ConstBytes(pinned[a].data_ptr(),
+                                                         len(shapes[a]["file"])),
+                MutableBytes(s["staging"].data_ptr(), s["need"].bytes), s["maps"], copy)
+            assert st == Status.success, st
+        staged = torch.cuda.Event()
+        staged.record(copy)
+        items = [(cuda.Operation.decode_calibrate, item_for(i, "direct")) for i in range(n)]
+        st, batch = cuda.prepare_mixed_batch(items, results, prep, graph=False)
+        assert st == Status.success, st
+        compute.wait_event(staged)
+        assert batch.run(compute) == Status.success
+        compute.synchronize()
+        copy.synchronize()
+        return [batch]
+
     def step(mode):
+        if mode == "direct_batched":
+            return step_batched()
         plans = []
         for i, (a, roi) in enumerate(reqs):
             s = slots[i]
@@ -1165,7 +1191,7 @@ def run_archive_roi(args, torch, shapes):
                        "sides log-uniform 128..2048, decode_calibrate to FP32 (offset 100.0, "
                        "gain 1.05), one plan per request",
            "mean_roi_mpx": round(px / n / 1e6, 3)}
-    for mode in ("direct", "gather", "whole_archive"):
+    for mode in ("direct", "direct_batched", "gather", "whole_archive"):
         step(mode)
         for k in host_us:
             host_us[k] = 0.0
@@ -1178,6 +1204,7 @@ def run_archive_roi(args, torch, shapes):
         recs = results.cpu().numpy().view(np.uint64).reshape(-1, 2)
         assert all(int(r[0]) == 0 for r in recs), recs[:4]
         h2d = {"direct": sum(s["need"].bytes for s in slots),
+               "direct_batched": sum(s["need"].bytes for s in slots),
                "gather": sum(s["gbytes"] for s in slots),
                "whole_archive": sum(len(shapes[a]["file"]) for a, _ in reqs)}[mode]
         out[mode] = {"ms_per_batch": round(sec * 1e3, 3), "requests_per_s": round(n / sec, 1),
