@@ -127,3 +127,72 @@ def test_out_of_order_payloads(cuda_ready, oracle_lib):
             want = frame[y:y + h, x:x + w]
             assert rec == (0, want.nbytes)
             assert np.array_equal(out.view(np.uint16).reshape(h, w), want)
+
+
+def test_staged_rois_as_one_mixed_batch(cuda_ready, oracle_lib):
+    """Several ROIs of uint16 and FP32 archives staged from pinned memory, then decoded as one
+    mixed batch (decode_roi and decode_calibrate items with their tile mappings): every output
+    equals the crop (or its calibrated form) of the source frame."""
+    t = torch()
+    rng = np.random.default_rng(37)
+    copy = t.cuda.Stream()
+    compute = t.cuda.current_stream()
+    items, keep, checks = [], [], []
+    for k, (ptype, tile) in enumerate([(oracle.UINT16, (128, 32)), (oracle.FLOAT32, (64, 64)),
+                                       (oracle.UINT16, (256, 16))]):
+        frame = (workloads.detector_frame(900, 500, 60 + k) if ptype == oracle.UINT16
+                 else workloads.field_frame(900, 500, 60 + k))
+        file = oracle_lib.compress_image(frame, tile)
+        st, meta = api.parse_metadata(np.frombuffer(file, dtype=np.uint8))
+        pinned = t.from_numpy(np.frombuffer(file, dtype=np.uint8).copy()).pin_memory()
+        keep += [meta, pinned]
+        for j in range(4):
+            x, y = int(rng.integers(0, 900)), int(rng.integers(0, 500))
+            roi = (x, y, int(rng.integers(1, 901 - x)), int(rng.integers(1, 501 - y)))
+            st, need = cuda.roi_staging_size(meta, Roi(*roi))
+            assert st == Status.success
+            staging = device_bytes(need.bytes)
+            maps = (TileMapping * need.tiles)()
+            st, _ = cuda.stage_roi_tiles(meta, Roi(*roi), ConstBytes(pinned.data_ptr(), len(file)),
+                                         MutableBytes(staging.data_ptr(), staging.numel()), maps,
+                                         copy)
+            assert st == Status.success, st
+            calibrated = j % 2 == 1
+            src = CompressedInput()
+            src.bytes = ConstBytes(staging.data_ptr(), need.bytes)
+            src.metadata = meta.handle
+            src.mappings = maps
+            src.mapping_count = need.tiles
+            x, y, w, h = roi
+            otype = api.PixelType.float32 if calibrated else api.PixelType(ptype)
+            s = api.sample_bytes(otype)
+            out = device_bytes(w * h * s)
+            item = BatchItem()
+            item.compressed_input = src
+            item.output = api.view(out, otype, w, h, w * s, out.numel())
+            item.roi = Roi(*roi)
+            if calibrated:
+                item.calibration = Calibration()
+                item.calibration.offset.scalar = 100.0
+                item.calibration.gain.scalar = 1.05
+            op = cuda.Operation.decode_calibrate if calibrated else cuda.Operation.decode_roi
+            items.append((op, item))
+            keep += [staging, maps, out]
+            region = np.ascontiguousarray(frame[y:y + h, x:x + w])
+            want = (oracle_lib.calibrate_image(region, 100.0, 1.05) if calibrated else region)
+            checks.append((out, want))
+    staged = t.cuda.Event()
+    staged.record(copy)
+    compute.wait_event(staged)
+    results = device_bytes(16 * len(items), fill=0xFF)
+    st, batch = cuda.prepare_mixed_batch(items, results, compute, graph=False)
+    assert st == Status.success, st
+    assert batch.run(compute) == Status.success
+    t.cuda.synchronize()
+    recs = host(results).view(np.uint64).reshape(-1, 2)
+    for k, (out, want) in enumerate(checks):
+        assert int(recs[k, 0]) == 0 and int(recs[k, 1]) == want.nbytes, k
+        got = host(out)[:want.nbytes].view(want.dtype).reshape(want.shape)
+        assert np.array_equal(got.view(np.uint8), want.view(np.uint8)) or (
+            want.dtype == np.float32 and np.all((got.view(np.uint32) == want.view(np.uint32)) |
+                                                (np.isnan(got) & np.isnan(want)))), k
