@@ -7,7 +7,8 @@
 * a 4096x4096 FP32 field (config 3's generator) encodes byte-identically and decodes bit-exact;
 * a config-4-sized mixed batch (sides 257..4096, uint16 and FP32, every tile shape, pitched
   input and output rows, calibration maps): every GPU-encoded file equals the oracle's, and every
-  output of one mixed batch equals the oracle's words (calibrated outputs its two-rounding form).
+  output of one mixed batch equals the oracle's words (calibrated outputs its two-rounding form);
+* all 256 archives of the benchmark's config-4 batch encode to the oracle's bytes.
 """
 import numpy as np
 import pytest
@@ -183,3 +184,30 @@ def test_config4_sized_mixed_batch(cuda_ready, oracle_lib):
                 assert f == oracle_lib.compress_image(words[k], tile), (k, tile)
                 files[k] = f
     _run_mixed(torch, stream, oracle_lib, rng, words, types, files)
+
+
+def test_config4_every_archive_encodes_to_oracle_bytes(cuda_ready, oracle_lib):
+    """All 256 archives of the benchmark's config-4 batch (bench.mixed_archives: sides uniform in
+    257..4096, 70% uint16 / 30% FP32, a random tile shape each, generated and encoded on the
+    GPU): every file equals the oracle's encoding of the same pixels, byte for byte."""
+    import concurrent.futures as cf
+
+    import bench
+    torch = cuda_ready
+    stream = torch.cuda.current_stream()
+    entries, plans, frames, keep, _, _ = bench.mixed_archives(torch, stream, 256)
+    torch.cuda.synchronize()
+
+    def check(k):
+        meta, src_dev = keep[3 * k], keep[3 * k + 1]
+        dev, w, h = frames[k]
+        pixels = dev.cpu().numpy()
+        img = pixels.view(np.uint16 if meta.image.type == 1 else np.uint32)
+        img = img.reshape(h, w) if meta.image.type == 1 else img.view(np.float32).reshape(h, w)
+        want = oracle_lib.compress_image(np.ascontiguousarray(img),
+                                         (meta.tile.width, meta.tile.height))
+        return src_dev.cpu().numpy().tobytes() == want
+
+    with cf.ThreadPoolExecutor(max_workers=8) as pool:
+        same = list(pool.map(check, range(256)))
+    assert all(same), [k for k, ok in enumerate(same) if not ok][:8]
