@@ -664,15 +664,16 @@ void pack(std::vector<std::uint8_t> &image, std::uint64_t at, const std::vector<
 }
 
 // Kernel shape of the plain uint16 decoder (see tsk_decode_config.shape and decode.cu's list).
-// The default, shape 13 (four consumer warps in two pairs, each pair decoding its own tiles,
-// 16 columns per lane, four stages, five CTAs per SM), measured fastest on B200;
-// TILESTREAM_DECODE_SHAPE overrides it for tuning runs.
+// The default, shape 15 (four warps in two pairs, each pair staging and decoding its own tiles
+// with no producer warp, 16 columns per lane, single-pass rows, two stages per pair, up to six
+// CTAs per SM), measured fastest on B200 over all the shapes; TILESTREAM_DECODE_SHAPE overrides
+// it for tuning runs.
 std::uint32_t decode_shape() {
     static const std::uint32_t shape = [] {
         const char *env = std::getenv("TILESTREAM_DECODE_SHAPE");
         return env != nullptr ? static_cast<std::uint32_t>(std::strtoul(env, nullptr, 10)) %
                                     TSK_DECODE_SHAPES
-                              : 13u;
+                              : 15u;
     }();
     return shape;
 }

@@ -1537,8 +1537,8 @@ __device__ __forceinline__ void decode_body_self(Source &source, const tsk_row_s
 
 // A planned queue (every plan and mixed batch); MinBlocks resident CTAs per SM.
 // Reserve: the kernel reserves all sixteen named barriers (named_sync_any), which holds an SM
-// to four resident CTAs; the default uint16 shape measured fastest so (faster than with five,
-// and than four enforced by padded shared memory).
+// to four resident CTAs; uint16 shape 13 measured fastest so (faster than with five, and than
+// four enforced by padded shared memory).
 template <uint32_t MaxPayload, uint32_t Stages, uint32_t Paths, uint32_t CW, uint32_t G16,
           uint32_t MinBlocks, uint32_t NR, uint32_t RW, bool Self, bool Dyn, bool Reserve>
 __global__ void __launch_bounds__(threads_of(CW, Self), MinBlocks)
@@ -1608,9 +1608,9 @@ Variant make() {
 // resident CTAs per SM in the launch bounds): 0 = 8 x 8, 4 stages, 4; 1 = 8 x 16, 4, 3;
 // 2 = 4 x 16, 4, 5; 3 = 4 x 8, 4, 6; 4 = 4 x 16, 4, 6 (64 registers); 5 = 4 x 16, 3, 7 (56
 // registers); 6 = 4 x 32, 4, 3; 7 = 4 x 32, 4, 4; 8-11 single-pass rows with one or two rows per
-// lane; 12-13 warps in groups of one or two per tile (13, the default: pairs, four CTAs per
-// SM); 14-17 without a producer warp (each group stages its own tiles); 18 = 13 with
-// the device work queue. The plain mixed uint16 + FP32 instance has ten: 0 = 8 x 8, 3 stages of
+// lane; 12-13 warps in groups of one or two per tile (13: pairs, four CTAs per SM); 14-17
+// without a producer warp (each group stages its own tiles; 15, the default: pairs, two stages
+// each, up to six CTAs per SM); 18 = 13 with the device work queue. The plain mixed uint16 + FP32 instance has ten: 0 = 8 x 8, 3 stages of
 // 16 KiB, 3 CTAs; 1 = 4 x 16, 2 stages, 5 CTAs; 2 = 4 x 16, 3, 4; 3 = 4 x 8, 2, 6 (two stages
 // leave shared memory for more resident CTAs); 4-7 variants of them with single-pass rows or
 // warp pairs; 8 and 9 = 5 and 6 with the device work queue. The other instances have shapes 0
