@@ -1141,12 +1141,13 @@ Status autotune(detail::PlanState &p, tsk_result *results, const char *cache, cu
         return detail::cuda_status(apply(hit->second.shape, hit->second.per_sm), "tuned config");
     }
     // The kernel shapes of the batch's instance (kernels/decode.cu, select): nineteen for plain
-    // uint16, ten for plain mixed uint16 + FP32, two for the others.
+    // uint16, twelve for plain mixed uint16 + FP32, two for the others.
     const bool plain_u16 = p.config.paths == (TSK_PATH_U16 | TSK_PATH_PLAIN);
     const bool plain_mixed = p.config.paths == (TSK_PATH_U16 | TSK_PATH_F32 | TSK_PATH_PLAIN);
     const std::uint32_t shapes_all[TSK_DECODE_SHAPES] = {0,  1,  2,  3,  4,  5,  6,  7,  8,  9,
                                                          10, 11, 12, 13, 14, 15, 16, 17, 18},
-                        shapes_mixed[] = {0, 1, 2, 3, 4, 5, 6, 7, 8, 9}, shapes_two[] = {0, 2};
+                        shapes_mixed[] = {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11},
+                        shapes_two[] = {0, 2};
     const std::uint32_t *shapes = plain_u16 ? shapes_all : plain_mixed ? shapes_mixed : shapes_two;
     const std::size_t nshapes = plain_u16 ? TSK_DECODE_SHAPES
                                 : plain_mixed ? sizeof(shapes_mixed) / sizeof(shapes_mixed[0])

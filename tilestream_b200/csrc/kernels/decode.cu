@@ -1610,11 +1610,13 @@ Variant make() {
 // registers); 6 = 4 x 32, 4, 3; 7 = 4 x 32, 4, 4; 8-11 single-pass rows with one or two rows per
 // lane; 12-13 warps in groups of one or two per tile (13: pairs, four CTAs per SM); 14-17
 // without a producer warp (each group stages its own tiles; 15, the default: pairs, two stages
-// each, up to six CTAs per SM); 18 = 13 with the device work queue. The plain mixed uint16 + FP32 instance has ten: 0 = 8 x 8, 3 stages of
-// 16 KiB, 3 CTAs; 1 = 4 x 16, 2 stages, 5 CTAs; 2 = 4 x 16, 3, 4; 3 = 4 x 8, 2, 6 (two stages
-// leave shared memory for more resident CTAs); 4-7 variants of them with single-pass rows or
-// warp pairs; 8 and 9 = 5 and 6 with the device work queue. The other instances have shapes 0
-// and 2 (odd shapes map to 0, even ones to 2), and single-pass rows from shape 8 on.
+// each, up to six CTAs per SM); 18 = 13 with the device work queue.
+// The plain mixed uint16 + FP32 instance has twelve: 0 = 8 x 8, 3 stages of 16 KiB, 3 CTAs;
+// 1 = 4 x 16, 2 stages, 5 CTAs; 2 = 4 x 16, 3, 4; 3 = 4 x 8, 2, 6 (two stages leave shared
+// memory for more resident CTAs); 4-7 variants of them with single-pass rows or warp pairs;
+// 8 and 9 = 5 and 6 with the device work queue; 10 and 11 without a producer warp.
+// The other instances have shapes 0 and 2 (odd shapes map to 0, even ones to 2), and
+// single-pass rows from shape 8 on.
 Variant select(uint32_t paths, uint32_t shape) {
     const bool f32 = paths & kF32, u16 = paths & kU16, plain = paths & kPlain, c = paths & kCal;
     const bool narrow = shape % 2 == 0 && shape != 0; // four consumer warps
@@ -1697,6 +1699,10 @@ Variant select(uint32_t paths, uint32_t shape) {
             return make<16384, 2, kU16 | kF32 | kPlain, 4, 16, 5, 1, 4, false, true>();
         case 9: // shape 6 with the device work queue
             return make<16384, 3, kU16 | kF32 | kPlain, 4, 16, 4, 1, 4, false, true>();
+        case 10: // no producer warp: one group of four warps staging its own tiles
+            return make<16384, 2, kU16 | kF32 | kPlain, 4, 16, 6, 1, 4, true>();
+        case 11: // no producer warp: two pairs, each staging its own tiles
+            return make<16384, 4, kU16 | kF32 | kPlain, 4, 16, 3, 1, 2, true>();
         default:
             return narrow ? make<16384, 3, kU16 | kF32 | kPlain, 4, 16, 4>()
                           : make<16384, 3, kU16 | kF32 | kPlain>();
