@@ -384,3 +384,26 @@ def test_tiles_larger_than_the_image_and_ragged_edges(tmp_path):
         st, got = api.read_tiff(path)
         assert st == Status.success and same_words(got["pixels"], img)
         assert same_words(np.array(Image.open(path)), img)
+
+
+def test_c_entry_points_refuse_null_arguments(tmp_path):
+    """The C layer's own argument checks: null outputs and handles are invalid_argument, and a
+    compression value outside the enum is refused before anything is written."""
+    img = u16_image(20, 10)
+    path = str(tmp_path / "c.tif")
+    assert N.lib().ts_read_tiff(os.fsencode(path), None, None) == Status.invalid_argument
+    spec, pitch, data, size = api.ImageSpec(), C.c_uint64(), C.c_void_p(), C.c_uint64()
+    assert N.lib().ts_tiff_image_pixels(None, C.byref(spec), C.byref(pitch), C.byref(data),
+                                        C.byref(size)) == Status.invalid_argument
+    N.lib().ts_tiff_image_destroy(None)  # a no-op
+    v = api.const_view(img, PixelType.uint16, 20, 10)
+    assert N.lib().ts_write_tiff(os.fsencode(path), v,
+                                 C.byref(TiffWriteOptions(0, 7, 0, 128, 32, 6))) == \
+        Status.invalid_argument
+    assert not os.path.exists(path)
+    assert api.write_tiff(path, img) == Status.success
+    st, h = read_handle(path)
+    assert st == Status.success
+    assert N.lib().ts_tiff_image_pixels(h, None, C.byref(pitch), C.byref(data),
+                                        C.byref(size)) == Status.invalid_argument
+    N.lib().ts_tiff_image_destroy(h)
