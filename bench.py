@@ -1849,7 +1849,11 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     line, shapes = run_ours(args, rank, world, local, torch, dist)
     if rank == 0:
-        sections = [s for s in args.sections.split(",") if s and s != "none"]
+        # The configs' sections, the host parse and the CPU baseline run at N = 1 only: a
+        # scaling run measures the headline step, and the other ranks would wait in the final
+        # barrier (whose timeout is short) while rank 0 ran them.
+        sections = [s for s in args.sections.split(",") if s and s != "none"] if world == 1 \
+            else []
         stream = torch.cuda.current_stream()
         peak = measured_peaks()[0]
         if "encode" in sections:
@@ -1862,8 +1866,11 @@ def main():
             line["serving"] = run_serving(args, torch, stream)
         if "archive_roi" in sections:
             line["archive_roi"] = run_archive_roi(args, torch, shapes)
-        line["host_parse"] = host_parse(shapes)
-        line["cpu_baseline"] = cpu_baseline(shapes, args.cpu_seconds)
+        if world == 1:
+            line["host_parse"] = host_parse(shapes)
+            line["cpu_baseline"] = cpu_baseline(shapes, args.cpu_seconds)
+        else:
+            line["cpu_baseline"] = None  # measured at N = 1
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
